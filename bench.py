@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Benchmark of the one-GPU collapsed-Gibbs LDA iteration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one full iteration (sample -> log-likelihood -> count rebuild) over
+the whole synthetic corpus.  The default workload is the 60M-token one
+(V=100k, D=300k, lognormal(5, 0.8) lengths, K=1024, alpha=50/1024, beta=0.01),
+generated from a seed; its working set (doc ids, topics, doc-reverse index,
+theta) is several times the 126 MB L2, so no flush is needed between steps.
+
+--impl ours (default): W untimed iterations, then K iterations timed with CUDA
+events on the sampler's stream, bracketed by a barrier and a synchronize; the
+max over ranks is reported.  Under torchrun each rank runs an independent
+replica (its own seed): the path has no exchange step on one GPU, so the
+scaling is weak and the value is the sum of tokens over ranks / max time.
+--impl reference: the reference's own CUDA build (oracle/_ref/culda, compiled
+from its sources for sm_100a) on the same corpus files, timed by its own
+per-iteration clock; rank 0 only.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "tokens/sec on 1 B200 (plain CGS)"
+UNIT = "tokens/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        exe = shutil.which("nvidia-smi")
+        if not exe:
+            return
+        self.proc = subprocess.Popen([exe, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                     stderr=subprocess.DEVNULL, text=True)
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- distributed
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    dev = "cuda" if torch.cuda.is_available() and pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cuda_sync():
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+    except Exception:
+        pass
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload: str):
+    """Sampler DRAM bytes per launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "sample_kernel_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------- ours
+def run_ours(args, world, rank, local, pg):
+    import ctypes as C
+
+    import numpy as np
+
+    import culda_cgs_b200 as cb
+    from culda_cgs_b200.configs import WORKLOADS
+
+    wl = WORKLOADS[args.workload].with_seed(args.seed + rank)
+    t0 = time.perf_counter()
+    corpus = cb.Corpus.generate(wl.gen)
+    log(f"[rank {rank}] corpus {wl.name}: D={corpus.num_docs} V={corpus.num_words} N={corpus.num_tokens} "
+        f"generated in {time.perf_counter() - t0:.1f}s")
+    N = corpus.num_tokens
+
+    # ---- device-resident measurement
+    m = cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed + rank, device=local, group_lanes=args.group_lanes,
+               item_tokens=args.item_tokens)
+    info = m.info()
+    log(f"[rank {rank}] info {info}")
+    warm = m.iterate(args.warmup) if args.warmup > 0 else []
+    barrier(pg)
+    cuda_sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    stats = m.iterate(args.steps)
+    cuda_sync()
+    barrier(pg)
+    clk = clocks.stop()
+    dev_seconds = sum(s["seconds"] for s in stats)
+    max_seconds = allreduce_max(pg, dev_seconds)
+    value = world * N * args.steps / max_seconds
+    for s in stats:
+        log(f"[rank {rank}] iteration {s['iteration']:4d}: {s['seconds'] * 1e3:8.3f} ms "
+            f"(sample {s['sample_seconds'] * 1e3:.3f} ms, rebuild {s['rebuild_seconds'] * 1e3:.3f} ms) "
+            f"loglik {s['loglik']:.6f}  {s['tokens_per_sec'] / 1e6:.1f} M tokens/s")
+
+    # ---- roofline of the sampler: algorithmic bytes per launch / event time
+    prev = ([warm[-1]] if warm else []) + stats[:-1]
+    if len(prev) < len(stats):  # no warm-up: the first sampler walked the initial rows
+        prev = [stats[0]] + prev
+    sample_bytes = [16 * N + 4 * p["token_nnz"] + 4 * info["num_hot_items"] * 0 for p in prev]
+    sample_sec = [s["sample_seconds"] for s in stats]
+    achieved = sum(sample_bytes) / sum(sample_sec) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic(args.workload)
+    roofline = {"kernel": "sample_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": traffic, "bytes_per_launch": int(statistics.mean(sample_bytes)),
+                "launch_ms": round(1e3 * statistics.mean(sample_sec), 4),
+                "rebuild_ms": round(1e3 * statistics.mean(s["rebuild_seconds"] for s in stats), 4),
+                "formula": "sum_t (4 doc id + 2 topic in + 2 topic out + 8 row) + 4 * sum_t nnz(row of d(t))"}
+    m.close()
+
+    # ---- end to end through the public API from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        import torch
+
+        cudart = torch.cuda.cudart()
+        c = corpus.c_ptr.contents
+        regs = [(C.cast(c.doc_ids, C.c_void_p).value, 4 * N), (C.cast(c.word_ptr, C.c_void_p).value,
+                8 * (corpus.num_words + 1)), (C.cast(c.doc_ptr, C.c_void_p).value, 8 * (corpus.num_docs + 1))]
+        for ptr, nbytes in regs:
+            cudart.cudaHostRegister(ptr, nbytes, 0)
+        z_host = torch.empty(N, dtype=torch.int16, pin_memory=True)
+        barrier(pg)
+        cuda_sync()
+        t0 = time.perf_counter()
+        m2 = cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed + rank, device=local,
+                    group_lanes=args.group_lanes, item_tokens=args.item_tokens)
+        lls = [s["loglik"] for s in m2.iterate(args.steps)]
+        st = cb.lib().culda_get_topics(m2._ctx, C.cast(z_host.data_ptr(), C.POINTER(C.c_uint16)))
+        cuda_sync()
+        t1 = time.perf_counter()
+        assert st == 0
+        m2.close()
+        for ptr, _ in regs:
+            cudart.cudaHostUnregister(ptr)
+        e2e_sec = allreduce_max(pg, t1 - t0)
+        h2d = 4 * N + 8 * (corpus.num_words + 1) + 8 * (corpus.num_docs + 1)
+        d2h = 2 * N + 64 * args.steps
+        e2e = {"value": world * N * args.steps / e2e_sec, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+               "seconds": round(e2e_sec, 4), "includes": "culda_create (upload, doc index sort, initial counts, "
+               "graph capture) + K iterations each reading its log-likelihood back + final topic download",
+               "loglik_last": lls[-1] if lls else None}
+
+    # ---- CPU baseline (rank 0, one GPU only): the OpenMP port of the same rule
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        t0 = time.perf_counter()
+        h = O.CpuCgs(corpus.doc_ptr, corpus.word_ptr, corpus.doc_ids, wl.k, wl.alpha, wl.beta, args.seed)
+        setup = time.perf_counter() - t0
+        secs = []
+        while len(secs) < args.cpu_iterations and sum(secs) < args.cpu_budget:
+            s, _ = h.iterate(1)
+            secs.append(float(s[0]))
+        cpu = {"value": N / statistics.mean(secs), "unit": UNIT, "cores": h.threads, "kind": "port",
+               "sample": f"iterations 1-{len(secs)} of a fresh chain on the full {N}-token corpus "
+                         f"(set-up {setup:.1f}s untimed); oracle/cgs_cpu.cpp, same sampling rule, FP32, OpenMP"}
+        h.close()
+
+    launches = info["kernels_per_iteration"] * args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * max_seconds / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded generator, shapes of the workload)",
+        "config": {"workload": wl.name, "num_tokens": N, "num_docs": corpus.num_docs, "num_words": corpus.num_words,
+                   "k": wl.k, "alpha": wl.alpha, "beta": wl.beta, "seed": args.seed,
+                   "group_lanes": info["group_lanes"], "items": info["num_items"], "hot_words": info["num_hot"],
+                   "l2": f"inputs larger than L2 (resident set {info['device_bytes'] / 1e9:.2f} GB > 126 MB)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        "loglik": [round(s["loglik"], 8) for s in stats],
+    }
+    return line
+
+
+# -------------------------------------------------------------- reference
+ITER_RE = re.compile(r"Iteration\s+(\d+):\s+([\d.]+) sec,\s+([\d.]+) sec, logLikelyhood = ([-\d.naninf]+),\s+([\d.]+) M")
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    binary = ROOT / "oracle" / "_ref" / "culda"
+    if not binary.exists():
+        return {"impl": "reference", "unavailable": "oracle/_ref/culda was not built (reference sources absent)"}
+    import culda_cgs_b200 as cb
+    from culda_cgs_b200.configs import WORKLOADS
+
+    wl = WORKLOADS[args.workload].with_seed(args.seed)
+    if wl.k != 1024:
+        return {"impl": "reference", "unavailable": "the reference kernel supports only K=1024"}
+    corpus = cb.Corpus.generate(wl.gen)
+    N = corpus.num_tokens
+    tmp = Path(tempfile.mkdtemp(prefix="culda_ref_"))
+    try:
+        corpus.write(str(tmp / "corpus"))
+        iters = args.warmup + args.steps
+        cmd = [str(binary), "-g", "1", "-c", "1", "-k", str(wl.k), "-t", str(iters), "-s", "1",
+               "-a", repr(float(wl.alpha)), "-b", repr(float(wl.beta)), "-i", str(tmp / "corpus")]
+        log("reference:", " ".join(cmd))
+        clocks = ClockSampler(0)
+        clocks.start()
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=args.ref_timeout)
+        clk = clocks.stop()
+        rows = [m.groups() for m in ITER_RE.finditer(r.stdout)]
+        if r.returncode != 0 or len(rows) < iters:
+            tail = (r.stdout + r.stderr)[-400:].replace("\n", " | ")
+            return {"impl": "reference", "unavailable": f"reference run failed (rc={r.returncode}): {tail}"}
+        for it, el, st, ll, mt in rows:
+            log(f"reference iteration {it}: {float(st) * 1e3:.1f} ms loglik {ll} {mt} M")
+        # the printed seconds have two decimals; the M tokens/s column has three
+        # significant decimals of a number in the hundreds, so derive each
+        # iteration's time from it
+        stamps = [N / (float(x[4]) * 1e6) for x in rows[args.warmup:iters]]
+        value = N * len(stamps) / sum(stamps)
+        return {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(stamps) / len(stamps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp16 phiHead / fp32 sums",
+            "data": "synthetic (seeded generator, shapes of the workload)",
+            "config": {"workload": wl.name, "num_tokens": N, "num_docs": corpus.num_docs,
+                       "num_words": corpus.num_words, "k": wl.k, "alpha": wl.alpha, "beta": wl.beta,
+                       "seed": args.seed, "parallelism": "single GPU",
+                       "timing": "the reference's own per-iteration host clock (SingleChunkSingleGPU.h:72-127)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"iterations {args.warmup + 1}-{iters} of the reference's CUDA build "
+                                       "(oracle/_ref/culda, sm_100a) on one B200, driven by one host thread"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clk, "loglik": [float(x[3]) for x in rows[args.warmup:iters]],
+        }
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="plain-cgs-scale")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--group-lanes", type=int, default=0)
+    ap.add_argument("--item-tokens", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-iterations", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work at most")
+    ap.add_argument("--ref-timeout", type=float, default=1200.0)
+    args = ap.parse_args()
+    if args.warmup < 0 or args.steps < 1:
+        ap.error("--steps >= 1 and --warmup >= 0")
+
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, world, rank)
+        else:
+            line = run_ours(args, world, rank, local, pg)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+"""Corpus in CuLDA_CGS's word-first format, backed by the C ABI.
+
+Mirrors the reference's `Document` (src_culda/model/doc.h:20-50):
+`Document.loadDocument(prefix, numChunks)` reads the src_format files and
+exposes numDocs / numWords / numTokens; the arrays are the reference's
+docIndices (doc_ptr), wordIndices (word_ptr) and wordTokens (doc_ids).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import check, lib
+
+
+@dataclass(frozen=True)
+class GenConfig:
+    """Parameters of the seeded synthetic LDA corpus (culda_gen_params)."""
+    num_words: int
+    num_topics: int
+    num_docs: int
+    len_law: int = _ffi.CULDA_LEN_POISSON
+    len_a: float = 100.0
+    len_b: float = 0.0
+    len_min: int = 10
+    len_max: int = 1000
+    zipf_s: float = 1.05
+    word_conc: float = 0.1
+    doc_conc: float = 0.1
+    seed: int = 1
+    threads: int = 0
+
+    def to_c(self) -> _ffi.GenParams:
+        return _ffi.GenParams(self.num_words, self.num_topics, self.num_docs, self.len_law, self.zipf_s,
+                              self.word_conc, self.doc_conc, self.len_a, self.len_b, self.len_min, self.len_max,
+                              self.seed, self.threads)
+
+
+class Corpus:
+    """A corpus owned by the library (culda_corpus)."""
+
+    def __init__(self, ptr: C.POINTER(_ffi.Corpus)):
+        self._ptr = ptr
+        c = ptr.contents
+        self.num_docs = int(c.num_docs)
+        self.num_words = int(c.num_words)
+        self.num_tokens = int(c.num_tokens)
+
+    # --- construction
+    @classmethod
+    def generate(cls, cfg: GenConfig) -> "Corpus":
+        out = C.POINTER(_ffi.Corpus)()
+        p = cfg.to_c()
+        check(lib().culda_corpus_generate(C.byref(p), C.byref(out)))
+        return cls(out)
+
+    @classmethod
+    def load(cls, prefix: str, num_chunks: int = 1) -> "Corpus":
+        out = C.POINTER(_ffi.Corpus)()
+        check(lib().culda_corpus_load(str(prefix).encode(), int(num_chunks), C.byref(out)))
+        return cls(out)
+
+    @classmethod
+    def from_arrays(cls, doc_ptr, word_ptr, doc_ids) -> "BorrowedCorpus":
+        return BorrowedCorpus(doc_ptr, word_ptr, doc_ids)
+
+    # --- I/O
+    def write(self, prefix: str, num_chunks: int = 1) -> None:
+        check(lib().culda_corpus_write(self._ptr, str(prefix).encode(), int(num_chunks)))
+
+    def write_text(self, path: str) -> None:
+        check(lib().culda_corpus_write_text(self._ptr, str(path).encode()))
+
+    # --- arrays (copies)
+    @property
+    def doc_ptr(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self._ptr.contents.doc_ptr, shape=(self.num_docs + 1,)).copy()
+
+    @property
+    def word_ptr(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self._ptr.contents.word_ptr, shape=(self.num_words + 1,)).copy()
+
+    @property
+    def doc_ids(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self._ptr.contents.doc_ids, shape=(self.num_tokens,)).copy()
+
+    def doc_tokens(self) -> np.ndarray:
+        """docRevIdx: word-major token ids grouped by doc (doc_chunk.cpp:225-255)."""
+        out = np.empty(self.num_tokens, dtype=np.int32)
+        check(lib().culda_corpus_doc_tokens(self._ptr, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out
+
+    @property
+    def doc_lengths(self) -> np.ndarray:
+        return np.diff(self.doc_ptr)
+
+    @property
+    def c_ptr(self):
+        return self._ptr
+
+    # reference spellings
+    @property
+    def numDocs(self) -> int:  # noqa: N802
+        return self.num_docs
+
+    @property
+    def numWords(self) -> int:  # noqa: N802
+        return self.num_words
+
+    @property
+    def numTokens(self) -> int:  # noqa: N802
+        return self.num_tokens
+
+    def close(self) -> None:
+        if self._ptr:
+            lib().culda_corpus_free(self._ptr)
+            self._ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BorrowedCorpus(Corpus):
+    """A corpus descriptor over caller-owned numpy arrays (not freed by the library)."""
+
+    def __init__(self, doc_ptr, word_ptr, doc_ids):
+        self._doc_ptr = np.ascontiguousarray(doc_ptr, dtype=np.int64)
+        self._word_ptr = np.ascontiguousarray(word_ptr, dtype=np.int64)
+        self._doc_ids = np.ascontiguousarray(doc_ids, dtype=np.int32)
+        self._c = _ffi.Corpus(len(self._doc_ptr) - 1, len(self._word_ptr) - 1, len(self._doc_ids),
+                              self._doc_ptr.ctypes.data_as(C.POINTER(C.c_int64)),
+                              self._word_ptr.ctypes.data_as(C.POINTER(C.c_int64)),
+                              self._doc_ids.ctypes.data_as(C.POINTER(C.c_int32)), None, 0)
+        super().__init__(C.pointer(self._c))
+
+    def close(self) -> None:
+        self._ptr = None
+
+
+class Document(Corpus):
+    """Reference spelling: Document().loadDocument(prefix, numChunks)."""
+
+    def __init__(self, ptr=None):
+        if ptr is not None:
+            super().__init__(ptr)
+        else:
+            self._ptr = None
+            self.num_docs = self.num_words = self.num_tokens = 0
+
+    def loadDocument(self, prefix: str, numChunks: int = 1) -> "Document":  # noqa: N802,N803
+        c = Corpus.load(prefix, numChunks)
+        self._ptr, c._ptr = c._ptr, None
+        Corpus.__init__(self, self._ptr)
+        return self

@@ -1,0 +1,719 @@
+// context.cu — the context API: device state of one corpus on one GPU, its
+// set-up, the iteration captured as CUDA graphs, and copy-out in the
+// reference's layouts.
+//
+// Replaces SingleChunkSingleGPU (src_culda/train/SingleChunkSingleGPU.h:5-157)
+// and the device-owning parts of DocChunk, ModelPhi/ModelPhiGPU and
+// ModelTheta/ModelThetaChunk.  One iteration is one graph launch:
+//   memset(work counter, hot rows) -> hot_rows -> sample(z[c] -> z[1-c])
+//   -> finalize_ll -> memset(n_k, stats) -> theta_rebuild(z[1-c])
+//   -> stats D2H (pinned)
+// Two graphs alternate the topic buffers (z is double-buffered so hot words
+// split over several CTAs read a stable snapshot while others write).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cub/device/device_radix_sort.cuh>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "philox.h"
+
+using namespace culda;
+
+struct culda_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    culda_params params{};
+    int32_t D = 0, V = 0, K = 0;
+    int64_t N = 0;
+    int group_lanes = 8;
+    int item_tokens = 0;
+
+    int64_t *d_word_ptr = nullptr, *d_doc_ptr = nullptr;
+    int32_t *d_doc_ids = nullptr, *d_doc_tok = nullptr, *d_doc_order = nullptr;
+    uint16_t *d_z[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint32_t *d_theta = nullptr;
+    int64_t theta_cap = 0;
+    int2 *d_rows = nullptr;
+    int32_t *d_nk = nullptr;
+    culda_item *d_items = nullptr, *d_hot_items = nullptr;
+    int32_t num_items = 0, num_hot_items = 0, num_hot = 0;
+    int32_t *d_hot_phi = nullptr;
+    double *d_item_ll = nullptr;
+    int32_t *d_counter = nullptr;
+    uint32_t *d_iter = nullptr;
+    DevStats *d_stats = nullptr;
+    int32_t *d_error = nullptr;
+    DevStats *h_stats = nullptr;  // pinned
+
+    int sample_grid = 1, theta_grid = 1;
+    double doc_term = 0;  // sum_d L_d * log(L_d + K alpha)
+    std::vector<int64_t> h_doc_ptr;
+    std::vector<int32_t> h_max_ia;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // recorded inside the iteration graph around the sampling and rebuild kernels
+    cudaEvent_t ev_s0 = nullptr, ev_s1 = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    uint32_t next_iteration = 1;
+    std::string err;
+};
+
+namespace {
+
+int fail(culda_ctx *c, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    set_global_error("%s", buf);
+    return code;
+}
+
+#define CK(call)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess)                                                                             \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? CULDA_ERR_OOM : CULDA_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                                \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T **p, size_t n) {
+    return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+}
+
+__global__ void iota_kernel(int64_t n, int32_t *v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = (int32_t)i;
+}
+
+__global__ void copy_error_kernel(const int32_t *err, DevStats *st) { st->error = *err; }
+
+int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
+    const int nxt = 1 - cur;
+    CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
+    if (ctx->num_hot > 0) {
+        CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
+        CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
+                           s));
+    }
+    CK(cudaEventRecord(ctx->ev_s0, s));
+    SampleParams p{};
+    p.k = ctx->K;
+    p.alpha = ctx->params.alpha;
+    p.beta = ctx->params.beta;
+    p.vbeta = ctx->params.beta * (float)ctx->V;
+    p.num_docs = ctx->D;
+    p.num_items = ctx->num_items;
+    p.num_hot = ctx->num_hot;
+    p.num_tokens = ctx->N;
+    p.theta_cap = ctx->theta_cap;
+    p.doc_ids = ctx->d_doc_ids;
+    p.topics_in = ctx->d_z[cur];
+    p.topics_out = ctx->d_z[nxt];
+    p.theta = ctx->d_theta;
+    p.rows = ctx->d_rows;
+    p.nk = ctx->d_nk;
+    p.items = ctx->d_items;
+    p.hot_phi = ctx->d_hot_phi;
+    p.item_counter = ctx->d_counter;
+    p.item_ll = ctx->d_item_ll;
+    p.seed = ctx->params.seed;
+    p.iteration = 0;
+    p.iteration_ptr = ctx->d_iter;
+    p.error = ctx->d_error;
+    CK(launch_sample(p, ctx->group_lanes, ctx->sample_grid, s));
+    CK(cudaEventRecord(ctx->ev_s1, s));
+    CK(launch_finalize_ll(ctx->d_item_ll, ctx->num_items, ctx->d_stats, ctx->d_iter, s));
+    CK(cudaMemsetAsync(ctx->d_nk, 0, sizeof(int32_t) * (size_t)ctx->K, s));
+    CK(cudaMemsetAsync(&ctx->d_stats->row_entries, 0, 3 * sizeof(int64_t), s));
+    CK(cudaEventRecord(ctx->ev_t0, s));
+    CK(launch_theta_rebuild(ctx->K, ctx->D, ctx->d_doc_ptr, ctx->d_doc_tok, ctx->d_z[nxt], ctx->d_doc_order,
+                            ctx->d_rows, ctx->d_theta, ctx->d_nk, &ctx->d_stats->row_entries, ctx->d_error,
+                            ctx->theta_grid, s));
+    CK(cudaEventRecord(ctx->ev_t1, s));
+    copy_error_kernel<<<1, 1, 0, s>>>(ctx->d_error, ctx->d_stats);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, s));
+    return CULDA_OK;
+}
+
+// Rebuild theta rows and n_k from the current topics (set-up and set_topics).
+int rebuild_counts(culda_ctx *ctx) {
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemsetAsync(ctx->d_nk, 0, sizeof(int32_t) * (size_t)ctx->K, s));
+    CK(cudaMemsetAsync(&ctx->d_stats->row_entries, 0, 3 * sizeof(int64_t), s));
+    CK(launch_theta_rebuild(ctx->K, ctx->D, ctx->d_doc_ptr, ctx->d_doc_tok, ctx->d_z[ctx->cur], ctx->d_doc_order,
+                            ctx->d_rows, ctx->d_theta, ctx->d_nk, &ctx->d_stats->row_entries, ctx->d_error,
+                            ctx->theta_grid, s));
+    CK(cudaStreamSynchronize(s));
+    int32_t e = 0;
+    CK(cudaMemcpy(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (e) return fail(ctx, CULDA_ERR_DEVICE_STATE, "theta rebuild reported device error 0x%x", e);
+    return CULDA_OK;
+}
+
+int build_graphs(culda_ctx *ctx) {
+    for (int c = 0; c < 2; ++c) {
+        if (ctx->graph[c]) {
+            cudaGraphExecDestroy(ctx->graph[c]);
+            ctx->graph[c] = nullptr;
+        }
+        if (ctx->params.flags & CULDA_FLAG_NO_GRAPH) continue;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = record_iteration(ctx, ctx->stream, c);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc != CULDA_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        CK(e);
+        e = cudaGraphInstantiate(&ctx->graph[c], g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+    }
+    return CULDA_OK;
+}
+
+int pick_group_lanes(int requested) {
+    if (requested == 1 || requested == 2 || requested == 4 || requested == 8 || requested == 16 || requested == 32)
+        return requested;
+    return requested == 0 ? 8 : -1;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- work items
+extern "C" int64_t culda_build_items(int32_t num_words, const int64_t *word_ptr, int32_t item_tokens,
+                                     culda_item *items, int64_t max_items, int32_t *num_hot) {
+    if (num_words <= 0 || !word_ptr || item_tokens <= 0) {
+        set_global_error("culda_build_items: invalid argument");
+        return CULDA_ERR_INVALID_ARG;
+    }
+    std::vector<culda_item> v;
+    int32_t hot = 0;
+    for (int32_t w = 0; w < num_words; ++w) {
+        const int64_t len = word_ptr[w + 1] - word_ptr[w];
+        if (len <= 0) continue;
+        if (len <= item_tokens) {
+            v.push_back(culda_item{word_ptr[w], (int32_t)len, w, -1, 1});
+        } else {
+            // slices of near-equal size, as the reference splits hot words
+            // into slots (doc_chunk.cpp:167-185)
+            const int64_t ns = (len + item_tokens - 1) / item_tokens, sz = (len + ns - 1) / ns;
+            for (int64_t i = 0; i < ns; ++i) {
+                const int64_t b = word_ptr[w] + i * sz, e = std::min(b + sz, word_ptr[w + 1]);
+                if (e > b) v.push_back(culda_item{b, (int32_t)(e - b), w, hot, i == 0 ? 1 : 0});
+            }
+            ++hot;
+        }
+    }
+    std::stable_sort(v.begin(), v.end(), [](const culda_item &a, const culda_item &b) { return a.count > b.count; });
+    if (num_hot) *num_hot = hot;
+    if (items) {
+        if ((int64_t)v.size() > max_items) {
+            set_global_error("culda_build_items: %zu items do not fit in %lld", v.size(), (long long)max_items);
+            return CULDA_ERR_INVALID_ARG;
+        }
+        std::copy(v.begin(), v.end(), items);
+    }
+    return (int64_t)v.size();
+}
+
+// --------------------------------------------------------------- create
+extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_ctx **out) {
+    culda_ctx *ctx = nullptr;
+    if (!c || !p || !out) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: null argument");
+    *out = nullptr;
+    if (p->k < 32 || p->k > 4096 || p->k % 32 != 0)
+        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: K=%d must be a multiple of 32 in [32, 4096]", p->k);
+    if (!(p->alpha > 0.f) || !(p->beta > 0.f) || !std::isfinite(p->alpha) || !std::isfinite(p->beta))
+        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: alpha and beta must be positive");
+    const int gl = pick_group_lanes(p->group_lanes);
+    if (gl < 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: group_lanes=%d", p->group_lanes);
+    if (c->num_docs <= 0 || c->num_words <= 0 || c->num_tokens <= 0 || !c->doc_ptr || !c->word_ptr || !c->doc_ids)
+        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: empty corpus");
+    if (c->num_tokens >= (int64_t)INT32_MAX)
+        return fail(ctx, CULDA_ERR_UNSUPPORTED, "culda_create: %lld tokens exceed the int32 token index",
+                    (long long)c->num_tokens);
+    if (c->doc_ptr[0] != 0 || c->word_ptr[0] != 0 || c->doc_ptr[c->num_docs] != c->num_tokens ||
+        c->word_ptr[c->num_words] != c->num_tokens)
+        return fail(ctx, CULDA_ERR_FORMAT, "culda_create: doc/word index totals do not match the token count");
+    for (int32_t d = 0; d < c->num_docs; ++d) {
+        const int64_t len = c->doc_ptr[d + 1] - c->doc_ptr[d];
+        if (len < 0) return fail(ctx, CULDA_ERR_FORMAT, "culda_create: doc index decreases at doc %d", d);
+        if (len > 65535)
+            return fail(ctx, CULDA_ERR_UNSUPPORTED, "culda_create: doc %d has %lld tokens (theta counts are 16-bit)", d,
+                        (long long)len);
+    }
+    for (int32_t w = 0; w < c->num_words; ++w)
+        if (c->word_ptr[w + 1] < c->word_ptr[w])
+            return fail(ctx, CULDA_ERR_FORMAT, "culda_create: word index decreases at word %d", w);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        return fail(ctx, CULDA_ERR_NO_DEVICE, "culda_create: no CUDA device");
+    if (p->device < 0 || p->device >= ndev)
+        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: device %d of %d", p->device, ndev);
+
+    ctx = new culda_ctx();
+    ctx->params = *p;
+    ctx->device = p->device;
+    ctx->D = c->num_docs;
+    ctx->V = c->num_words;
+    ctx->K = p->k;
+    ctx->N = c->num_tokens;
+    ctx->group_lanes = gl;
+    int rc = CULDA_OK;
+    auto bail = [&](int code) {
+        culda_destroy(ctx);
+        return code;
+    };
+#define CKB(call)                                                                                              \
+    do {                                                                                                       \
+        cudaError_t e_ = (call);                                                                               \
+        if (e_ != cudaSuccess) {                                                                               \
+            fail(ctx, e_ == cudaErrorMemoryAllocation ? CULDA_ERR_OOM : CULDA_ERR_CUDA, "%s: %s", #call,       \
+                 cudaGetErrorString(e_));                                                                      \
+            set_global_error("%s", ctx->err.c_str());                                                          \
+            return bail(e_ == cudaErrorMemoryAllocation ? CULDA_ERR_OOM : CULDA_ERR_CUDA);                     \
+        }                                                                                                      \
+    } while (0)
+
+    CKB(cudaSetDevice(ctx->device));
+    CKB(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CKB(cudaEventCreate(&ctx->ev0));
+    CKB(cudaEventCreate(&ctx->ev1));
+    CKB(cudaEventCreate(&ctx->ev_s0));
+    CKB(cudaEventCreate(&ctx->ev_s1));
+    CKB(cudaEventCreate(&ctx->ev_t0));
+    CKB(cudaEventCreate(&ctx->ev_t1));
+    cudaStream_t s = ctx->stream;
+    const int64_t N = ctx->N;
+    const int32_t D = ctx->D, V = ctx->V, K = ctx->K;
+
+    // corpus upload
+    CKB(dalloc(&ctx->d_word_ptr, (size_t)V + 1));
+    CKB(dalloc(&ctx->d_doc_ptr, (size_t)D + 1));
+    CKB(dalloc(&ctx->d_doc_ids, (size_t)N));
+    CKB(cudaMemcpyAsync(ctx->d_word_ptr, c->word_ptr, sizeof(int64_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, s));
+    CKB(cudaMemcpyAsync(ctx->d_doc_ptr, c->doc_ptr, sizeof(int64_t) * ((size_t)D + 1), cudaMemcpyHostToDevice, s));
+    CKB(cudaMemcpyAsync(ctx->d_doc_ids, c->doc_ids, sizeof(int32_t) * (size_t)N, cudaMemcpyHostToDevice, s));
+    CKB(dalloc(&ctx->d_error, 64));
+    CKB(cudaMemsetAsync(ctx->d_error, 0, 64 * sizeof(int32_t), s));
+
+    // doc ids in range and doc lengths consistent with the payload
+    {
+        int32_t *d_cnt = nullptr;
+        CKB(dalloc(&d_cnt, (size_t)D));
+        CKB(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (size_t)D, s));
+        CKB(launch_doc_check(N, D, ctx->d_doc_ids, d_cnt, ctx->d_error, s));
+        std::vector<int32_t> cnt((size_t)D);
+        int32_t e = 0;
+        CKB(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int32_t) * (size_t)D, cudaMemcpyDeviceToHost, s));
+        CKB(cudaMemcpyAsync(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CKB(cudaStreamSynchronize(s));
+        cudaFree(d_cnt);
+        if (e) {
+            fail(ctx, CULDA_ERR_FORMAT, "culda_create: a doc id is outside [0, %d)", D);
+            return bail(CULDA_ERR_FORMAT);
+        }
+        for (int32_t d = 0; d < D; ++d)
+            if (cnt[d] != c->doc_ptr[d + 1] - c->doc_ptr[d]) {
+                fail(ctx, CULDA_ERR_FORMAT, "culda_create: doc %d has %d tokens in the payload but length %lld", d,
+                     cnt[d], (long long)(c->doc_ptr[d + 1] - c->doc_ptr[d]));
+                return bail(CULDA_ERR_FORMAT);
+            }
+    }
+
+    // doc-reverse index: stable radix sort of token ids by doc id
+    // (the reference builds it on the host, doc_chunk.cpp:225-255)
+    {
+        CKB(dalloc(&ctx->d_doc_tok, (size_t)N));
+        int32_t *keys_out = nullptr, *vals_in = nullptr;
+        CKB(dalloc(&keys_out, (size_t)N));
+        CKB(dalloc(&vals_in, (size_t)N));
+        iota_kernel<<<1024, 256, 0, s>>>(N, vals_in);
+        CKB(cudaGetLastError());
+        int end_bit = 1;
+        while ((1ll << end_bit) < (int64_t)D) ++end_bit;
+        size_t tmp_bytes = 0;
+        CKB(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok,
+                                            (int)N, 0, end_bit, s));
+        void *tmp = nullptr;
+        CKB(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 1)));
+        CKB(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok, (int)N,
+                                            0, end_bit, s));
+        CKB(cudaStreamSynchronize(s));
+        cudaFree(tmp);
+        cudaFree(keys_out);
+        cudaFree(vals_in);
+    }
+
+    // theta layout: capacity roundup32(min(L_d, K)) per doc (model_theta.cpp:50-56)
+    ctx->h_doc_ptr.assign(c->doc_ptr, c->doc_ptr + D + 1);
+    ctx->h_max_ia.resize((size_t)D + 1);
+    std::vector<int2> rows((size_t)D);
+    int64_t off = 0;
+    for (int32_t d = 0; d < D; ++d) {
+        int64_t len = c->doc_ptr[d + 1] - c->doc_ptr[d];
+        if (len > K) len = K;
+        len = (len + 31) / 32 * 32;
+        if (off + len >= (int64_t)INT32_MAX) {
+            fail(ctx, CULDA_ERR_UNSUPPORTED, "culda_create: theta capacity exceeds int32 offsets");
+            return bail(CULDA_ERR_UNSUPPORTED);
+        }
+        ctx->h_max_ia[d] = (int32_t)off;
+        rows[d] = make_int2((int)off, (int)off);
+        off += len;
+        ctx->doc_term += (double)(c->doc_ptr[d + 1] - c->doc_ptr[d]) *
+                         std::log((double)(c->doc_ptr[d + 1] - c->doc_ptr[d]) + (double)K * (double)p->alpha);
+    }
+    ctx->h_max_ia[D] = (int32_t)off;
+    ctx->theta_cap = off;
+    CKB(dalloc(&ctx->d_theta, (size_t)off));
+    CKB(cudaMemsetAsync(ctx->d_theta, 0, sizeof(uint32_t) * (size_t)std::max<int64_t>(off, 1), s));
+    CKB(dalloc(&ctx->d_rows, (size_t)D));
+    CKB(cudaMemcpyAsync(ctx->d_rows, rows.data(), sizeof(int2) * (size_t)D, cudaMemcpyHostToDevice, s));
+
+    // docs longest first for the theta rebuild's warps
+    {
+        std::vector<int32_t> order((size_t)D);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+            return c->doc_ptr[a + 1] - c->doc_ptr[a] > c->doc_ptr[b + 1] - c->doc_ptr[b];
+        });
+        CKB(dalloc(&ctx->d_doc_order, (size_t)D));
+        CKB(cudaMemcpyAsync(ctx->d_doc_order, order.data(), sizeof(int32_t) * (size_t)D, cudaMemcpyHostToDevice, s));
+        CKB(cudaStreamSynchronize(s));
+    }
+
+    // grids
+    const int sms = num_sms(ctx->device);
+    int sbps = sample_blocks_per_sm(K, gl);
+    if (sbps <= 0) {
+        fail(ctx, CULDA_ERR_CUDA, "culda_create: sampler does not fit on the device for K=%d", K);
+        return bail(CULDA_ERR_CUDA);
+    }
+    int tbps = theta_blocks_per_sm(K);
+    if (tbps <= 0) tbps = 1;
+    ctx->theta_grid = std::max(1, std::min(sms * tbps, (D + kThetaWarps - 1) / kThetaWarps));
+
+    // work items: words, hot words split so no item exceeds a quarter of a CTA's share
+    {
+        int64_t it = p->item_tokens;
+        if (it <= 0) it = std::max<int64_t>(1024, std::min<int64_t>(65535, N / ((int64_t)sms * sbps * 4)));
+        ctx->item_tokens = (int)it;
+        int32_t nhot = 0;
+        const int64_t n_items = culda_build_items(V, c->word_ptr, ctx->item_tokens, nullptr, 0, &nhot);
+        if (n_items <= 0 || n_items >= INT32_MAX) {
+            fail(ctx, CULDA_ERR_FORMAT, "culda_create: no tokens to sample");
+            return bail(CULDA_ERR_FORMAT);
+        }
+        std::vector<culda_item> items((size_t)n_items), hot;
+        culda_build_items(V, c->word_ptr, ctx->item_tokens, items.data(), n_items, &nhot);
+        for (const culda_item &x : items)
+            if (x.hot >= 0) hot.push_back(x);
+        ctx->num_items = (int32_t)n_items;
+        ctx->num_hot = nhot;
+        ctx->num_hot_items = (int32_t)hot.size();
+        CKB(dalloc(&ctx->d_items, items.size()));
+        CKB(cudaMemcpyAsync(ctx->d_items, items.data(), sizeof(culda_item) * items.size(), cudaMemcpyHostToDevice, s));
+        CKB(dalloc(&ctx->d_hot_items, hot.size()));
+        if (!hot.empty())
+            CKB(cudaMemcpyAsync(ctx->d_hot_items, hot.data(), sizeof(culda_item) * hot.size(), cudaMemcpyHostToDevice,
+                                s));
+        CKB(dalloc(&ctx->d_hot_phi, (size_t)nhot * K));
+        CKB(dalloc(&ctx->d_item_ll, (size_t)n_items));
+        CKB(cudaStreamSynchronize(s));
+    }
+    ctx->sample_grid = std::max(1, std::min(ctx->num_items, sms * sbps));
+
+    CKB(dalloc(&ctx->d_counter, 64));
+    CKB(dalloc(&ctx->d_iter, 1));
+    CKB(dalloc(&ctx->d_stats, 1));
+    CKB(dalloc(&ctx->d_nk, (size_t)K));
+    CKB(cudaMallocHost((void **)&ctx->h_stats, sizeof(DevStats)));
+    memset(ctx->h_stats, 0, sizeof(DevStats));
+    CKB(cudaMemsetAsync(ctx->d_stats, 0, sizeof(DevStats), s));
+    const uint32_t one = 1;
+    CKB(cudaMemcpyAsync(ctx->d_iter, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+
+    // topics: Philox init, then the initial counts (SingleChunkSingleGPU.h:24-41)
+    CKB(dalloc(&ctx->d_z[0], (size_t)N));
+    CKB(dalloc(&ctx->d_z[1], (size_t)N));
+    CKB(launch_init_topics(N, K, p->seed, ctx->d_z[0], s));
+    ctx->cur = 0;
+    rc = rebuild_counts(ctx);
+    if (rc) return bail(rc);
+    rc = build_graphs(ctx);
+    if (rc) return bail(rc);
+    if (p->flags & CULDA_FLAG_VERBOSE)
+        fprintf(stderr,
+                "culda: D=%d V=%d N=%lld K=%d items=%d hot_words=%d hot_items=%d item_tokens=%d theta_cap=%lld "
+                "sample_grid=%d theta_grid=%d G=%d\n",
+                D, V, (long long)N, K, ctx->num_items, ctx->num_hot, ctx->num_hot_items, ctx->item_tokens,
+                (long long)ctx->theta_cap, ctx->sample_grid, ctx->theta_grid, gl);
+    *out = ctx;
+    return CULDA_OK;
+#undef CKB
+}
+
+// -------------------------------------------------------------- iterate
+extern "C" int culda_iterate(culda_ctx *ctx, int n, culda_iter_stats *stats) {
+    if (!ctx || n < 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_iterate: invalid argument");
+    CK(cudaSetDevice(ctx->device));
+    for (int i = 0; i < n; ++i) {
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        if (ctx->graph[ctx->cur]) {
+            CK(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+        } else {
+            int rc = record_iteration(ctx, ctx->stream, ctx->cur);
+            if (rc) return rc;
+        }
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        CK(cudaEventSynchronize(ctx->ev1));
+        float ms = 0.f, ms_s = 0.f, ms_t = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        CK(cudaEventElapsedTime(&ms_s, ctx->ev_s0, ctx->ev_s1));
+        CK(cudaEventElapsedTime(&ms_t, ctx->ev_t0, ctx->ev_t1));
+        ctx->cur = 1 - ctx->cur;
+        const DevStats h = *ctx->h_stats;
+        ctx->next_iteration = h.iteration + 1;
+        if (stats) {
+            culda_iter_stats &o = stats[i];
+            o.iteration = (int32_t)h.iteration;
+            o.status = h.error;
+            o.seconds = ms * 1e-3;
+            o.loglik = (h.ll_sum - ctx->doc_term) / (double)ctx->N;
+            o.tokens_per_sec = ms > 0 ? (double)ctx->N / (ms * 1e-3) : 0.0;
+            o.row_entries = h.row_entries;
+            o.theta_nnz = h.nnz;
+            o.token_nnz = h.token_nnz;
+            o.sample_seconds = ms_s * 1e-3;
+            o.rebuild_seconds = ms_t * 1e-3;
+        }
+        if (h.error) return fail(ctx, CULDA_ERR_DEVICE_STATE, "iteration %u: device error word 0x%x", h.iteration, h.error);
+    }
+    return CULDA_OK;
+}
+
+extern "C" int culda_set_topics(culda_ctx *ctx, const uint16_t *topics) {
+    if (!ctx || !topics) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_set_topics: null argument");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->d_z[ctx->cur], topics, sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    return rebuild_counts(ctx);
+}
+
+extern "C" int culda_get_topics(culda_ctx *ctx, uint16_t *topics) {
+    if (!ctx) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_get_topics: null context");
+    CK(cudaSetDevice(ctx->device));
+    if (topics) {
+        CK(cudaMemcpyAsync(topics, ctx->d_z[ctx->cur], sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return CULDA_OK;
+}
+
+extern "C" int culda_get_phi(culda_ctx *ctx, int32_t *phi, int32_t *nk) {
+    if (!ctx) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_get_phi: null context");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    if (phi) {
+        int32_t *d_phi = nullptr, *d_nk2 = nullptr;
+        CK(dalloc(&d_phi, (size_t)ctx->V * ctx->K));
+        CK(dalloc(&d_nk2, (size_t)ctx->K));
+        CK(cudaMemsetAsync(d_nk2, 0, sizeof(int32_t) * (size_t)ctx->K, s));
+        CK(launch_update_phi(ctx->K, ctx->V, ctx->d_word_ptr, ctx->d_z[ctx->cur], d_phi, d_nk2, ctx->d_error, s));
+        CK(cudaMemcpyAsync(phi, d_phi, sizeof(int32_t) * (size_t)ctx->V * ctx->K, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        cudaFree(d_phi);
+        cudaFree(d_nk2);
+    }
+    if (nk) {
+        CK(cudaMemcpyAsync(nk, ctx->d_nk, sizeof(int32_t) * (size_t)ctx->K, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    return CULDA_OK;
+}
+
+extern "C" int culda_get_theta(culda_ctx *ctx, int16_t *theta_a, int16_t *theta_ja, int32_t *max_ia,
+                               int32_t *cur_ia) {
+    if (!ctx) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_get_theta: null context");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    if (theta_a || theta_ja) {
+        std::vector<uint32_t> t((size_t)ctx->theta_cap);
+        CK(cudaMemcpyAsync(t.data(), ctx->d_theta, sizeof(uint32_t) * t.size(), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < t.size(); ++i) {
+            if (theta_a) theta_a[i] = (int16_t)(uint16_t)(t[i] >> 16);
+            if (theta_ja) theta_ja[i] = (int16_t)(uint16_t)(t[i] & 0xFFFFu);
+        }
+    }
+    if (max_ia) std::copy(ctx->h_max_ia.begin(), ctx->h_max_ia.end(), max_ia);
+    if (cur_ia) {
+        std::vector<int2> r((size_t)ctx->D);
+        CK(cudaMemcpyAsync(r.data(), ctx->d_rows, sizeof(int2) * r.size(), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (int32_t d = 0; d < ctx->D; ++d) cur_ia[d] = r[d].y;
+    }
+    return CULDA_OK;
+}
+
+extern "C" int64_t culda_theta_capacity(const culda_ctx *ctx) { return ctx ? ctx->theta_cap : -1; }
+extern "C" int64_t culda_num_tokens(const culda_ctx *ctx) { return ctx ? ctx->N : -1; }
+
+extern "C" int culda_sample_snapshot(culda_ctx *ctx, uint32_t iteration, uint16_t *topics_out, double *loglik) {
+    if (!ctx) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_sample_snapshot: null context");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const int cur = ctx->cur, nxt = 1 - cur;
+    CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
+    if (ctx->num_hot > 0) {
+        CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
+        CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
+                           s));
+    }
+    SampleParams p{};
+    p.k = ctx->K;
+    p.alpha = ctx->params.alpha;
+    p.beta = ctx->params.beta;
+    p.vbeta = ctx->params.beta * (float)ctx->V;
+    p.num_docs = ctx->D;
+    p.num_items = ctx->num_items;
+    p.num_hot = ctx->num_hot;
+    p.num_tokens = ctx->N;
+    p.theta_cap = ctx->theta_cap;
+    p.doc_ids = ctx->d_doc_ids;
+    p.topics_in = ctx->d_z[cur];
+    p.topics_out = ctx->d_z[nxt];
+    p.theta = ctx->d_theta;
+    p.rows = ctx->d_rows;
+    p.nk = ctx->d_nk;
+    p.items = ctx->d_items;
+    p.hot_phi = ctx->d_hot_phi;
+    p.item_counter = ctx->d_counter;
+    p.item_ll = ctx->d_item_ll;
+    p.seed = ctx->params.seed;
+    p.iteration = iteration;
+    p.iteration_ptr = nullptr;
+    p.error = ctx->d_error;
+    CK(launch_sample(p, ctx->group_lanes, ctx->sample_grid, s));
+    CK(launch_finalize_ll(ctx->d_item_ll, ctx->num_items, ctx->d_stats, nullptr, s));
+    DevStats h{};
+    int32_t e = 0;
+    CK(cudaMemcpyAsync(&h, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    if (topics_out)
+        CK(cudaMemcpyAsync(topics_out, ctx->d_z[nxt], sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (loglik) *loglik = (h.ll_sum - ctx->doc_term) / (double)ctx->N;
+    if (e) return fail(ctx, CULDA_ERR_DEVICE_STATE, "sampler reported device error 0x%x", e);
+    return CULDA_OK;
+}
+
+extern "C" int culda_loglik_joint(culda_ctx *ctx, double *ll) {
+    if (!ctx || !ll) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_loglik_joint: null argument");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const int P = num_sms(ctx->device) * 4;
+    double *d_part = nullptr;
+    CK(dalloc(&d_part, (size_t)P));
+    CK(launch_loglik_joint(ctx->K, ctx->V, ctx->D, ctx->params.alpha, ctx->params.beta, ctx->d_word_ptr,
+                           ctx->d_z[ctx->cur], ctx->d_rows, ctx->d_theta, ctx->d_doc_ptr, ctx->d_nk, d_part, P,
+                           ctx->d_error, s));
+    std::vector<double> part((size_t)P);
+    std::vector<int32_t> nk((size_t)ctx->K);
+    CK(cudaMemcpyAsync(part.data(), d_part, sizeof(double) * (size_t)P, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(nk.data(), ctx->d_nk, sizeof(int32_t) * (size_t)ctx->K, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    cudaFree(d_part);
+    const double a = ctx->params.alpha, b = ctx->params.beta, vb = (double)ctx->V * b, ka = (double)ctx->K * a;
+    double sum = 0, comp = 0;
+    auto add = [&](double x) {
+        const double t = sum + x;
+        if (std::fabs(sum) >= std::fabs(x))
+            comp += (sum - t) + x;
+        else
+            comp += (x - t) + sum;
+        sum = t;
+    };
+    for (double x : part) add(x);
+    add((double)ctx->K * std::lgamma(vb));
+    for (int32_t k : nk) add(-std::lgamma((double)k + vb));
+    add((double)ctx->D * std::lgamma(ka));
+    *ll = sum + comp;
+    return CULDA_OK;
+}
+
+extern "C" int culda_get_info(const culda_ctx *ctx, culda_info *info) {
+    if (!ctx || !info) return CULDA_ERR_INVALID_ARG;
+    info->num_items = ctx->num_items;
+    info->num_hot = ctx->num_hot;
+    info->num_hot_items = ctx->num_hot_items;
+    info->item_tokens = ctx->item_tokens;
+    info->group_lanes = ctx->group_lanes;
+    info->sample_grid = ctx->sample_grid;
+    info->theta_grid = ctx->theta_grid;
+    // hot_rows (when words are split), sample, finalize_ll, theta_rebuild, copy_error
+    info->kernels_per_iteration = (ctx->num_hot > 0 ? 1 : 0) + 4;
+    info->theta_capacity = ctx->theta_cap;
+    const int64_t N = ctx->N, D = ctx->D, V = ctx->V, K = ctx->K;
+    info->device_bytes = 8 * (V + 1) + 8 * (D + 1) + 4 * N /*doc ids*/ + 4 * N /*doc_tok*/ + 4 * D /*order*/ +
+                         2 * 2 * N /*topics*/ + 4 * ctx->theta_cap + 8 * D /*rows*/ + 4 * K +
+                         (int64_t)sizeof(culda_item) * (ctx->num_items + ctx->num_hot_items) +
+                         4 * (int64_t)ctx->num_hot * K + 8 * (int64_t)ctx->num_items;
+    info->doc_term = ctx->doc_term;
+    return CULDA_OK;
+}
+
+extern "C" const char *culda_last_error(const culda_ctx *ctx) { return ctx ? ctx->err.c_str() : global_error(); }
+
+extern "C" void culda_destroy(culda_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int c = 0; c < 2; ++c)
+        if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
+    void *bufs[] = {ctx->d_word_ptr, ctx->d_doc_ptr, ctx->d_doc_ids,  ctx->d_doc_tok,  ctx->d_doc_order,
+                    ctx->d_z[0],     ctx->d_z[1],    ctx->d_theta,    ctx->d_rows,     ctx->d_nk,
+                    ctx->d_items,    ctx->d_hot_items, ctx->d_hot_phi, ctx->d_item_ll, ctx->d_counter,
+                    ctx->d_iter,     ctx->d_stats,   ctx->d_error};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+    for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->ev_s0, ctx->ev_s1, ctx->ev_t0, ctx->ev_t1})
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" const char *culda_status_string(int status) {
+    switch (status) {
+        case CULDA_OK: return "ok";
+        case CULDA_ERR_INVALID_ARG: return "invalid argument";
+        case CULDA_ERR_IO: return "i/o error";
+        case CULDA_ERR_FORMAT: return "format error";
+        case CULDA_ERR_CUDA: return "CUDA error";
+        case CULDA_ERR_OOM: return "out of memory";
+        case CULDA_ERR_UNSUPPORTED: return "unsupported";
+        case CULDA_ERR_DEVICE_STATE: return "inconsistent device state";
+        case CULDA_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+extern "C" const char *culda_version(void) { return "culda-b200 0.1 sm_100a"; }

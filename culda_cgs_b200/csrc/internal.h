@@ -1,0 +1,29 @@
+// internal.h — declarations shared by the library's translation units.
+#pragma once
+#include <stdarg.h>
+#include <stdint.h>
+
+#include "../../include/culda_b200.h"
+
+namespace culda {
+
+// Thread-local message of the last failed call that has no context.
+void set_global_error(const char *fmt, ...);
+const char *global_error();
+
+// Host checks of a corpus descriptor (prefix arrays, doc ids, doc lengths).
+int validate_corpus(const culda_corpus *c);
+
+// Device error word bits.
+enum : int32_t {
+    kErrTopicRange = 1,   // a topic >= K was found in the topic array
+    kErrDocRange = 2,     // a doc id outside [0, D) reached the sampler
+    kErrRowRange = 4,     // a theta row outside the theta array or misaligned
+    kErrLongDoc = 8       // a document longer than 65535 tokens
+};
+
+// Sampler block size and the dynamic shared memory it needs for K topics.
+constexpr int kSampleThreads = 128;
+constexpr int kThetaWarps = 8;
+
+}  // namespace culda

@@ -1,0 +1,326 @@
+/*
+ * culda_b200.h — C ABI of the B200-native collapsed-Gibbs LDA sampler.
+ *
+ * This library is a drop-in for CuLDA_CGS's one-GPU path (`culda -g 1 -c 1`):
+ * the per-iteration sample -> log-likelihood -> phi/n_k rebuild -> theta rebuild
+ * loop.  Every entry point is `extern "C"`, takes plain pointers and sizes,
+ * never throws, never calls exit(), and returns an int status (0 = ok,
+ * negative = error; see CULDA_* below).  Host buffers belong to the caller;
+ * device buffers created by culda_create belong to the context.
+ *
+ * Two layers are exported:
+ *   1. Context API (culda_create / culda_iterate / culda_get_*): replaces the
+ *      reference driver SingleChunkSingleGPU (src_culda/train/SingleChunkSingleGPU.h:5-157)
+ *      together with the classes that own device memory there
+ *      (DocChunk, ModelPhi/ModelPhiGPU, ModelTheta/ModelThetaChunk).
+ *   2. Kernel-level API (culda_update_phi, culda_compute_phi_head,
+ *      culda_update_theta, culda_sample, culda_loglik): device pointers owned by
+ *      the caller, one entry point per reference kernel API, so a maintainer can
+ *      swap them in call by call.  Each cites the reference function it replaces.
+ *
+ * Layout conventions (all little-endian, device arrays unless stated):
+ *   word_ptr  int64[V+1]  token range of each word in word-major order
+ *                         (reference: wordIndices, doc_chunk.cpp:118-134)
+ *   doc_ids   int32[N]    doc id of every token, word-major, ascending within a
+ *                         word (reference: wordTokens, the .word.data payload)
+ *   topics    uint16[N]   topic of every token (reference: wordTopics, int16)
+ *   doc_ptr   int64[D+1]  token count prefix per doc (reference: docRevIndices)
+ *   doc_tok   int32[N]    word-major token index of every token, grouped by doc
+ *                         and ascending within a doc (reference: docRevIdx)
+ *   theta     uint32[cap] packed CSR entry (count << 16) | topic, ascending
+ *                         topic inside a row, zero padded (reference: thetaA and
+ *                         thetaJA, two int16 arrays, lda_theta_kernel.cu:55-58)
+ *   theta_rows int32[2*D] {row start, row end} per doc; start is the reference's
+ *                         thetaMaxIA[d], end its thetaCurIA[d] = start + roundup32(nnz)
+ *   nk        int32[K]    tokens per topic (reference: phiTopic)
+ *   phi       int32[V*K]  word-topic counts, row per word (reference: phiTopicWord)
+ */
+#ifndef CULDA_B200_H_
+#define CULDA_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; exactly the entry points
+ * declared here are exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum {
+    CULDA_OK = 0,
+    CULDA_ERR_INVALID_ARG = -1,  /* bad argument or size                       */
+    CULDA_ERR_IO = -2,           /* file missing or unreadable                 */
+    CULDA_ERR_FORMAT = -3,       /* file contents inconsistent                 */
+    CULDA_ERR_CUDA = -4,         /* a CUDA runtime call failed                 */
+    CULDA_ERR_OOM = -5,          /* host or device allocation failed           */
+    CULDA_ERR_UNSUPPORTED = -6,  /* valid input outside what this build runs   */
+    CULDA_ERR_DEVICE_STATE = -7, /* a kernel found an inconsistent state       */
+    CULDA_ERR_NO_DEVICE = -8     /* no CUDA device visible                     */
+};
+
+/* Human-readable name of a status code (static storage). */
+const char *culda_status_string(int status);
+
+/* Library version string, e.g. "culda-b200 0.1 sm_100a". */
+const char *culda_version(void);
+
+/* ------------------------------------------------------------------ corpus */
+/*
+ * Host-side corpus in CuLDA_CGS's word-first format (src_format/format.cpp:64-157,
+ * src_format/data_chunk.h:49-67): a doc index, a word index and the word-major
+ * doc-id payload.  A corpus returned by culda_corpus_load/generate owns its
+ * arrays and is released with culda_corpus_free; a caller may also fill the
+ * struct with its own arrays (then it must not call culda_corpus_free on it).
+ */
+typedef struct culda_corpus {
+    int32_t num_docs;   /* D */
+    int32_t num_words;  /* V */
+    int64_t num_tokens; /* N */
+    int64_t *doc_ptr;   /* [D+1], doc_ptr[0] = 0 (the .doc.idx cumulative ends)  */
+    int64_t *word_ptr;  /* [V+1], word_ptr[0] = 0 (the .word.idx cumulative ends) */
+    int32_t *doc_ids;   /* [N] word-major doc ids (the .word.data payload)        */
+    int32_t *word_label;/* [V] or NULL: token string of word v is "w<label>"      */
+    int32_t owned;      /* 1 when the arrays belong to the library                */
+} culda_corpus;
+
+enum { CULDA_LEN_POISSON = 0, CULDA_LEN_LOGNORMAL = 1, CULDA_LEN_PARETO = 2 };
+
+/* Seeded synthetic LDA corpus (no reference counterpart; stands in for the
+ * reference's unnamed datasets).  Topic-word distributions phi_k ~ Dir(word_conc * V * p)
+ * with p_r proportional to r^-zipf_s; doc mixtures theta_d ~ Dir(doc_conc) over
+ * num_topics; doc lengths from len_law clipped to [len_min, len_max].  Word ids
+ * are assigned by first appearance, as src_format/format.cpp:75-76 does. */
+typedef struct culda_gen_params {
+    int32_t num_words;
+    int32_t num_topics;
+    int32_t num_docs;
+    int32_t len_law;    /* CULDA_LEN_* */
+    double zipf_s;
+    double word_conc;
+    double doc_conc;
+    double len_a;       /* poisson: lambda; lognormal: mu; pareto: shape */
+    double len_b;       /* lognormal: sigma; pareto: x_m                 */
+    int32_t len_min;
+    int32_t len_max;
+    uint64_t seed;
+    int32_t threads;    /* host threads, 0 = all                         */
+} culda_gen_params;
+
+int culda_corpus_generate(const culda_gen_params *p, culda_corpus **out);
+
+/* Read `<prefix>.doc.idx`, `.chunk`, `.word.idx`, `.word.data` exactly as
+ * Document::loadDocument (src_culda/model/doc.cpp:62-156) and
+ * DocChunk::loadChunk (src_culda/model/doc_chunk.cpp:106-223) do.  Only
+ * num_chunks == 1 is supported (the one-GPU path); the .chunk file must hold
+ * exactly num_chunks rows (doc.cpp:111-114). */
+int culda_corpus_load(const char *prefix, int num_chunks, culda_corpus **out);
+
+/* Write the five src_format files for `c` (byte-identical to what
+ * src_format/format.cpp writes for the equivalent text corpus). */
+int culda_corpus_write(const culda_corpus *c, const char *prefix, int num_chunks);
+
+/* Write the corpus as text, one doc per line "d<id> w<label> w<label> ...",
+ * the input format of src_format/format.cpp. */
+int culda_corpus_write_text(const culda_corpus *c, const char *path);
+
+void culda_corpus_free(culda_corpus *c);
+
+/* doc_tok[N] (reference docRevIdx, doc_chunk.cpp:225-255) on the host. */
+int culda_corpus_doc_tokens(const culda_corpus *c, int32_t *doc_tok);
+
+/* ------------------------------------------------------------------ context */
+typedef struct culda_params {
+    int32_t k;            /* topics: multiple of 32, 32..4096 (reference: -k, rounded up to 32 in main.cpp:132-135) */
+    float alpha;          /* reference: -a */
+    float beta;           /* reference: -b */
+    uint64_t seed;        /* Philox key for init and sampling */
+    int32_t device;       /* CUDA device ordinal */
+    int32_t group_lanes;  /* lanes per token in the sampler: 0 = auto, else 1,2,4,8,16,32 */
+    int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto */
+    int32_t flags;        /* CULDA_FLAG_* */
+} culda_params;
+
+enum {
+    CULDA_FLAG_NO_GRAPH = 1,      /* launch the iteration kernel by kernel instead of one CUDA graph */
+    CULDA_FLAG_VERBOSE = 2        /* print set-up details to stderr */
+};
+
+typedef struct culda_iter_stats {
+    int32_t iteration;      /* 1-based */
+    int32_t status;         /* device error word after the iteration (0 = consistent) */
+    double seconds;         /* device time of the iteration (CUDA events) */
+    double loglik;          /* mean log((S+Q)/(L_d+K*alpha)) over tokens, pre-sampling snapshot
+                               (the reference's printed value, lda_train_kernel.cu:258, without
+                               its per-warp int truncation) */
+    double tokens_per_sec;  /* N / seconds */
+    int64_t row_entries;    /* sum over tokens of the padded theta row length of the rebuilt state */
+    int64_t theta_nnz;      /* non-zeros in theta after the rebuild */
+    int64_t token_nnz;      /* sum over tokens of the non-zeros in their doc's rebuilt row */
+    double sample_seconds;  /* device time of the sampler kernel */
+    double rebuild_seconds; /* device time of the theta / n_k rebuild */
+} culda_iter_stats;
+
+typedef struct culda_ctx culda_ctx;
+
+/* Upload the corpus, build the doc-reverse index, the theta layout and the
+ * sampler work list, draw the initial topics (Philox, counter (t, 0, 0, 1))
+ * and build the initial counts.  Replaces DocChunk::allocGPU/toGPU
+ * (doc_chunk.cpp:277-356), Document::generateTopics (doc_chunk.cpp:259-264),
+ * ModelPhi::InitData/UpdatePhiGPU/UpdatePhiHead and ModelTheta::InitData/
+ * UpdateThetaGPU (SingleChunkSingleGPU.h:15-41). */
+int culda_create(const culda_corpus *c, const culda_params *p, culda_ctx **out);
+
+/* Run n iterations (sample, log-likelihood, rebuild counts), one CUDA graph
+ * launch each, writing one culda_iter_stats per iteration into stats (may be
+ * NULL).  Replaces the loop body SingleChunkSingleGPU.h:70-127. */
+int culda_iterate(culda_ctx *ctx, int n, culda_iter_stats *stats);
+
+/* Replace all topics from a host array and rebuild the counts. */
+int culda_set_topics(culda_ctx *ctx, const uint16_t *topics);
+
+/* Copy state back (reference: DocChunk::toCPU, ModelPhi::MasterGPUToCPU,
+ * ModelTheta::toCPU, SingleChunkSingleGPU.h:138-148).  Any pointer may be NULL. */
+int culda_get_topics(culda_ctx *ctx, uint16_t *topics);
+int culda_get_phi(culda_ctx *ctx, int32_t *phi, int32_t *nk);
+/* thetaA / thetaJA in the reference's two-int16 layout, plus MaxIA[D+1] and CurIA[D]. */
+int culda_get_theta(culda_ctx *ctx, int16_t *theta_a, int16_t *theta_ja, int32_t *max_ia, int32_t *cur_ia);
+int64_t culda_theta_capacity(const culda_ctx *ctx);
+int64_t culda_num_tokens(const culda_ctx *ctx);
+
+/* One sampling pass over the current snapshot with Philox counter `iteration`,
+ * without rebuilding counts or advancing the iteration counter; writes the
+ * sampled topics (host, may be NULL) and the snapshot log-likelihood.  Used to
+ * compare a single draw with the host oracle on a frozen snapshot. */
+int culda_sample_snapshot(culda_ctx *ctx, uint32_t iteration, uint16_t *topics_out, double *loglik);
+
+/* FP64 joint log-likelihood log p(w, z) of the current state (Griffiths and
+ * Steyvers 2004, lgamma form).  No reference counterpart. */
+int culda_loglik_joint(culda_ctx *ctx, double *ll);
+
+/* Layout and launch facts of a context (no reference counterpart). */
+typedef struct culda_info {
+    int32_t num_items;          /* sampler work items */
+    int32_t num_hot;            /* words split over several items */
+    int32_t num_hot_items;
+    int32_t item_tokens;        /* largest item */
+    int32_t group_lanes;        /* lanes per token in the sampler */
+    int32_t sample_grid;        /* persistent sampler CTAs */
+    int32_t theta_grid;         /* theta rebuild CTAs */
+    int32_t kernels_per_iteration;
+    int64_t theta_capacity;     /* theta entries */
+    int64_t device_bytes;       /* device memory held by the context */
+    double doc_term;            /* sum_d L_d log(L_d + K alpha) */
+} culda_info;
+
+int culda_get_info(const culda_ctx *ctx, culda_info *info);
+
+const char *culda_last_error(const culda_ctx *ctx);
+void culda_destroy(culda_ctx *ctx);
+
+/* ------------------------------------------------------------- kernel level */
+/* A sampler work item: tokens [begin, begin+count) of one word.  Words with
+ * more than item_tokens tokens are split into several items (hot words; the
+ * reference's slots, doc_chunk.cpp:148-205); `hot` indexes their phi row in
+ * the hot-row buffer, -1 for words held by a single item. */
+typedef struct culda_item {
+    int64_t begin;
+    int32_t count;
+    int32_t word;
+    int32_t hot;
+    int32_t first;  /* 1 on the first item of its word */
+} culda_item;
+
+/* Build the work list for `word_ptr` (host).  Items are ordered largest first.
+ * Returns the number of items (<= max_items) or a negative status; with
+ * items == NULL only counts.  *num_hot receives the number of hot words. */
+int64_t culda_build_items(int32_t num_words, const int64_t *word_ptr, int32_t item_tokens,
+                          culda_item *items, int64_t max_items, int32_t *num_hot);
+
+/* Replaces LDAUpdatePhiAPI (src_culda/kernel/lda_phi_kernel.cu:136-159) and the
+ * n_k memset before it (src_culda/model/model_phi_gpu.cpp:79).  Per-word shared
+ * memory histograms, no global atomics and no per-warp scratch array; nk is
+ * the column sum of phi. */
+int culda_update_phi(int32_t k, int32_t num_words, const int64_t *d_word_ptr, const uint16_t *d_topics,
+                     int32_t *d_phi, int32_t *d_nk, void *stream);
+
+/* Replaces LDAComputePhiHeadAPI (src_culda/kernel/lda_phi_kernel.cu:49-72):
+ * phi_head[w*K+k] = (phi[w*K+k] + beta) / (nk[k] + V*beta) in FP32 (the
+ * reference rounds it to FP16).  The sampler computes this on the fly; this
+ * entry point exists for callers that want the table. */
+int culda_compute_phi_head(int32_t k, float beta, int32_t num_words, const int32_t *d_phi, const int32_t *d_nk,
+                           float *d_phi_head, void *stream);
+
+/* Workspace bytes culda_update_theta needs for num_docs documents. */
+size_t culda_update_theta_workspace(int32_t k, int32_t num_docs);
+
+/* Replaces LDAUpdateThetaAPI (src_culda/kernel/lda_theta_kernel.cu:89-126) and
+ * the two memsets before it (src_culda/model/model_theta_chunk.cpp:114-115).
+ * Rebuilds every theta row from the topics of its doc's tokens, writes
+ * theta_rows[2d+1] (the row end) and zeroes the part of the old row past the
+ * new end; d_nk (optional) receives the topic totals.  d_doc_order lists the
+ * docs longest first (length binning); NULL means 0..D-1.  d_stats (optional,
+ * int64[3]) receives {sum_d L_d * rowlen_d, sum_d nnz_d, sum_d L_d * nnz_d}. */
+int culda_update_theta(int32_t k, int32_t num_docs, const int64_t *d_doc_ptr, const int32_t *d_doc_tok,
+                       const uint16_t *d_topics, const int32_t *d_doc_order, int32_t *d_theta_rows,
+                       uint32_t *d_theta, int32_t *d_nk, int64_t *d_stats, void *d_workspace,
+                       size_t workspace_bytes, void *stream);
+
+typedef struct culda_sample_args {
+    int32_t k;
+    float alpha;
+    float beta;
+    int32_t num_docs;
+    int32_t num_words;
+    int64_t num_tokens;
+    const int64_t *word_ptr;     /* [V+1] */
+    const int32_t *doc_ids;      /* [N] */
+    const uint16_t *topics_in;   /* [N] topics of the snapshot: phi rows are histogrammed from them */
+    uint16_t *topics_out;        /* [N] sampled topics (must not alias topics_in) */
+    const uint32_t *theta;       /* packed CSR of the snapshot */
+    const int32_t *theta_rows;   /* [2*D] */
+    const int32_t *nk;           /* [K] of the snapshot */
+    const culda_item *items;     /* device copy of the work list */
+    int32_t num_items;
+    int32_t num_hot;             /* words split over several items */
+    const culda_item *hot_items; /* device copy of the items with hot >= 0 (any order) */
+    int32_t num_hot_items;
+    int64_t theta_capacity;      /* entries in theta (rows are checked against it) */
+    uint64_t seed;
+    uint32_t iteration;          /* Philox counter word 2 */
+    int32_t group_lanes;         /* 1,2,4,8,16,32 */
+    double *loglik_sum;          /* device double: receives sum over tokens of log(S+Q) */
+    int32_t *error;              /* device int32 error word (optional) */
+} culda_sample_args;
+
+/* Workspace bytes culda_sample needs (hot phi rows, per-item partial sums). */
+size_t culda_sample_workspace(int32_t k, int32_t num_items, int32_t num_hot);
+
+/* Replaces the LDAKernelTrain launch (src_culda/kernel/lda_train_kernel.cu:20-271,
+ * launched at src_culda/train/SingleChunkSingleGPU.h:75-100) and the per-token
+ * log terms it writes.  For every token t of word w in doc d on the frozen
+ * snapshot: S = sum_k theta_dk * phihat_wk over the doc's row, Q = alpha *
+ * sum_k phihat_wk, u = Philox4x32-10(key=seed, ctr={t_lo, t_hi, iteration, 0}),
+ * draw by inverse CDF over the row (ascending topic) then over 0..K-1. */
+int culda_sample(const culda_sample_args *a, void *d_workspace, size_t workspace_bytes, void *stream);
+
+/* Replaces LDATrainPerplexity (src_culda/kernel/lda_train_kernel.cu:323-356):
+ * turns the device sum written by culda_sample into the per-token value the
+ * reference prints: (sum - sum_d L_d*log(L_d + K*alpha)) / N, read back to
+ * host (synchronises the stream). */
+int culda_loglik(const double *d_loglik_sum, double doc_term, int64_t num_tokens, double *loglik, void *stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CULDA_B200_H_ */

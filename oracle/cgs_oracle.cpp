@@ -1,0 +1,409 @@
+/*
+ * cgs_oracle.cpp — TEST INFRASTRUCTURE ONLY.
+ *
+ * Host FP64 restatement of CuLDA_CGS's one-GPU iteration, used as the checker
+ * for the CUDA path.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg may load this library; the product never links or calls it.
+ *
+ * What it restates (reference paths relative to the CuLDA_CGS tree):
+ *   - doc-reverse index          src_culda/model/doc_chunk.cpp:225-255
+ *   - theta row capacities       src_culda/model/model_theta.cpp:50-56,
+ *                                src_culda/model/model_theta_chunk.cpp:74-85
+ *   - phi / n_k counts           src_culda/kernel/lda_phi_kernel.cu:94-116
+ *   - phiHead (FP16 table)       src_culda/kernel/lda_phi_kernel.cu:24-30
+ *   - theta CSR compaction       src_culda/kernel/lda_theta_kernel.cu:33-85
+ *   - sampling rule and buckets  src_culda/kernel/lda_train_kernel.cu:65-259
+ *   - per-token log term         src_culda/kernel/lda_train_kernel.cu:258
+ *   - validPhi / validTheta      src_culda/model/model_phi.cpp:194-280,
+ *                                src_culda/model/model_theta_chunk.cpp:142-273
+ * and two parts with no reference counterpart: the Philox4x32-10 counter RNG
+ * (Salmon, Moraes, Dror, Shaw, "Parallel Random Numbers: As Easy as 1, 2, 3",
+ * SC'11) and the Griffiths-Steyvers joint log-likelihood.
+ *
+ * Parity pins: Philox against the published known-answer vectors; counts,
+ * theta layout and phiHead against outputs of the reference's own kernels
+ * (tests/golden/, made by tests/golden/make_golden.py); the sampling rule and
+ * the per-token log term are restated from the kernel source (the reference
+ * draws from cuRAND XORWOW seeded by clock(), so its topic draws cannot be
+ * replayed).
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+extern "C" {
+
+/* ---------------------------------------------------------------- Philox */
+/* Philox4x32-10 from the SC'11 paper: 10 rounds of the 4x32 S-box with
+ * multipliers 0xD2511F53 / 0xCD9E8D57 and a Weyl key schedule
+ * 0x9E3779B9 / 0xBB67AE85. */
+void oracle_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+static inline uint32_t philox_word0(uint64_t seed, uint64_t t, uint32_t iter, uint32_t purpose) {
+    uint32_t ctr[4] = {(uint32_t)t, (uint32_t)(t >> 32), iter, purpose};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t out[4];
+    oracle_philox4x32_10(ctr, key, out);
+    return out[0];
+}
+
+/* Uniform in (0,1): (2*(x>>9)+1) * 2^-24, exact in float and double. */
+double oracle_uniform(uint32_t x) { return (double)((((x >> 9) << 1) | 1u)) * 0x1p-24; }
+
+/* Initial topics: z_t = floor(x0 * K / 2^32) with x0 = Philox(seed, {t, 0, 1}).
+ * (The reference draws rand() % K after srand(time(NULL)), doc_chunk.cpp:259-264.) */
+void oracle_init_topics(int64_t n, int32_t k, uint64_t seed, uint16_t *z) {
+    for (int64_t t = 0; t < n; ++t) {
+        uint32_t x = philox_word0(seed, (uint64_t)t, 0u, 1u);
+        z[t] = (uint16_t)(((uint64_t)x * (uint64_t)k) >> 32);
+    }
+}
+
+/* ------------------------------------------------------------- structure */
+/* docRevIdx: the word-major token ids of each doc in ascending order
+ * (doc_chunk.cpp:225-255). */
+void oracle_doc_rev(int32_t num_docs, int64_t n, const int32_t *doc_ids, const int64_t *doc_ptr, int32_t *doc_tok) {
+    std::vector<int64_t> cur(doc_ptr, doc_ptr + num_docs);
+    for (int64_t t = 0; t < n; ++t) doc_tok[cur[doc_ids[t]]++] = (int32_t)t;
+}
+
+/* thetaMaxIA: row capacity roundup32(min(L_d, K)), rows back to back
+ * (model_theta.cpp:50-56, model_theta_chunk.cpp:74-85). Returns the total. */
+int64_t oracle_theta_layout(int32_t num_docs, int32_t k, const int64_t *doc_ptr, int32_t *max_ia) {
+    int64_t off = 0;
+    for (int32_t d = 0; d < num_docs; ++d) {
+        int64_t len = doc_ptr[d + 1] - doc_ptr[d];
+        if (len >= k) len = k;
+        len = (len + 31) / 32 * 32;
+        max_ia[d] = (int32_t)off;
+        off += len;
+    }
+    max_ia[num_docs] = (int32_t)off;
+    return off;
+}
+
+/* phi[w*K+k] and n_k (lda_phi_kernel.cu:94-116). */
+void oracle_phi_counts(int32_t num_words, int32_t k, const int64_t *word_ptr, const uint16_t *z, int32_t *phi,
+                       int32_t *nk) {
+    std::memset(nk, 0, sizeof(int32_t) * (size_t)k);
+    for (int32_t w = 0; w < num_words; ++w) {
+        int32_t *row = phi + (size_t)w * k;
+        std::memset(row, 0, sizeof(int32_t) * (size_t)k);
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) {
+            row[z[t]]++;
+            nk[z[t]]++;
+        }
+    }
+}
+
+/* IEEE binary16 round-to-nearest-even of a float, from the format definition. */
+uint16_t oracle_float_to_half(float f) {
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    uint32_t sign = (x >> 16) & 0x8000u;
+    uint32_t exp = (x >> 23) & 0xFFu;
+    uint32_t man = x & 0x7FFFFFu;
+    if (exp == 0xFFu) return (uint16_t)(sign | 0x7C00u | (man ? 0x200u : 0u));
+    int32_t e = (int32_t)exp - 127 + 15;
+    if (e >= 31) return (uint16_t)(sign | 0x7C00u);
+    if (e <= 0) {
+        if (e < -10) return (uint16_t)sign;
+        uint32_t m = man | 0x800000u;
+        uint32_t shift = (uint32_t)(14 - e);
+        uint32_t half_m = m >> shift;
+        uint32_t rem = m & ((1u << shift) - 1u);
+        uint32_t halfway = 1u << (shift - 1);
+        if (rem > halfway || (rem == halfway && (half_m & 1u))) half_m++;
+        return (uint16_t)(sign | half_m);
+    }
+    uint32_t h = sign | ((uint32_t)e << 10) | (man >> 13);
+    uint32_t rem = man & 0x1FFFu;
+    if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) h++;
+    return (uint16_t)h;
+}
+
+float oracle_half_to_float(uint16_t h) {
+    uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+    uint32_t exp = (h >> 10) & 0x1Fu;
+    uint32_t man = h & 0x3FFu;
+    uint32_t x;
+    if (exp == 0) {
+        if (man == 0) {
+            x = sign;
+        } else {
+            int e = -1;
+            do {
+                man <<= 1;
+                ++e;
+            } while (!(man & 0x400u));
+            x = sign | ((uint32_t)(127 - 15 - e) << 23) | ((man & 0x3FFu) << 13);
+        }
+    } else if (exp == 31) {
+        x = sign | 0x7F800000u | (man << 13);
+    } else {
+        x = sign | ((exp - 15 + 127) << 23) | (man << 13);
+    }
+    float f;
+    std::memcpy(&f, &x, 4);
+    return f;
+}
+
+/* The reference's FP16 phiHead (lda_phi_kernel.cu:26-29): the quotient is
+ * formed in float, (phi + beta) / (n_k + beta * V), then rounded to half. */
+void oracle_phi_head_f16(int32_t num_words, int32_t k, float beta, const int32_t *phi, const int32_t *nk,
+                         uint16_t *out) {
+    for (int32_t w = 0; w < num_words; ++w)
+        for (int32_t j = 0; j < k; ++j) {
+            volatile float num = (float)phi[(size_t)w * k + j] + beta;
+            volatile float den = (float)nk[j] + beta * (float)num_words;
+            volatile float q = num / den;
+            out[(size_t)w * k + j] = oracle_float_to_half(q);
+        }
+}
+
+/* Theta CSR (lda_theta_kernel.cu:33-85): for each doc, the histogram of its
+ * tokens' topics, non-zeros in ascending topic order from thetaMaxIA[d],
+ * thetaCurIA[d] = start + roundup32(nnz); entries past nnz up to the row
+ * capacity are zero (the memsets at model_theta_chunk.cpp:114-115). */
+void oracle_theta_csr(int32_t num_docs, int32_t k, const int64_t *doc_ptr, const int32_t *doc_tok,
+                      const uint16_t *z, const int32_t *max_ia, int16_t *theta_a, int16_t *theta_ja,
+                      int32_t *cur_ia) {
+    std::vector<int32_t> dense((size_t)k);
+    for (int32_t d = 0; d < num_docs; ++d) {
+        std::fill(dense.begin(), dense.end(), 0);
+        for (int64_t i = doc_ptr[d]; i < doc_ptr[d + 1]; ++i) dense[z[doc_tok[i]]]++;
+        int32_t start = max_ia[d], cap_end = max_ia[d + 1], nnz = 0;
+        for (int32_t j = start; j < cap_end; ++j) {
+            theta_a[j] = 0;
+            theta_ja[j] = 0;
+        }
+        for (int32_t j = 0; j < k; ++j)
+            if (dense[j] > 0) {
+                theta_a[start + nnz] = (int16_t)dense[j];
+                theta_ja[start + nnz] = (int16_t)j;
+                ++nnz;
+            }
+        cur_ia[d] = start + (nnz + 31) / 32 * 32;
+    }
+}
+
+/* Host recount checks of validPhi (model_phi.cpp:194-280) and validTheta
+ * (model_theta_chunk.cpp:142-273), generalised from the hard-coded K = 1024.
+ * Return 0 when consistent, else a positive code naming the first failed check. */
+int oracle_valid_phi(int32_t num_words, int32_t k, const int64_t *word_ptr, const uint16_t *z, const int32_t *phi,
+                     const int32_t *nk) {
+    std::vector<int32_t> row((size_t)k), tot((size_t)k, 0);
+    for (int32_t w = 0; w < num_words; ++w) {
+        std::fill(row.begin(), row.end(), 0);
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) {
+            if (z[t] >= k) return 3;
+            row[z[t]]++;
+            tot[z[t]]++;
+        }
+        for (int32_t j = 0; j < k; ++j)
+            if (row[j] != phi[(size_t)w * k + j]) return 1;
+    }
+    for (int32_t j = 0; j < k; ++j)
+        if (tot[j] != nk[j]) return 2;
+    return 0;
+}
+
+int oracle_valid_theta(int32_t num_docs, int32_t k, const int64_t *doc_ptr, const int32_t *doc_tok, const uint16_t *z,
+                       const int16_t *theta_a, const int16_t *theta_ja, const int32_t *max_ia, const int32_t *cur_ia) {
+    std::vector<int32_t> dense((size_t)k), mask((size_t)k);
+    for (int32_t d = 0; d < num_docs; ++d) {
+        int32_t s = max_ia[d], e = max_ia[d + 1];
+        if (s % 32 != 0 || e % 32 != 0) return 1; /* rows 32-aligned */
+        int found = 0;
+        for (int32_t j = s; j < e; ++j)
+            if (theta_ja[j] == 0 && theta_a[j] != 0) {
+                if (found) return 2; /* topic 0 at most once */
+                found = 1;
+            }
+        std::fill(dense.begin(), dense.end(), 0);
+        std::fill(mask.begin(), mask.end(), 0);
+        for (int64_t i = doc_ptr[d]; i < doc_ptr[d + 1]; ++i) dense[z[doc_tok[i]]]++;
+        for (int32_t j = s; j < e; ++j) {
+            if (theta_a[j] == 0) continue;
+            mask[theta_ja[j]] = 1;
+            /* thetaA is int16 in the reference: compare in that width */
+            if ((int16_t)dense[theta_ja[j]] != theta_a[j]) return 3; /* non-zero entry disagrees with the recount */
+        }
+        for (int32_t j = 0; j < k; ++j)
+            if (!mask[j] && dense[j] != 0) return 4; /* topic missing from the row */
+        /* the used region ends at start + roundup32(nnz) */
+        int32_t nnz = 0;
+        for (int32_t j = 0; j < k; ++j) nnz += dense[j] > 0;
+        if (cur_ia[d] != s + (nnz + 31) / 32 * 32) return 5;
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- sampling */
+/*
+ * One sampling pass on a frozen snapshot in FP64 (lda_train_kernel.cu:65-259
+ * restated).  For token t of word w in doc d:
+ *   phihat_k = (n_wk + beta) / (n_k + V*beta)        (lda_phi_kernel.cu:26, in FP64)
+ *   S = sum over the doc's row, ascending topic, of A_i * phihat_{JA_i}
+ *   Q = alpha * sum_{k=0}^{K-1} phihat_k
+ *   u = uniform(Philox(seed, {t_lo, t_hi, iteration, 0}).x0)
+ *   T = u * (S + Q); T < S picks the first row entry whose running sum
+ *   exceeds T, otherwise the first topic whose running alpha*phihat sum
+ *   exceeds T - S.  (The reference tests u < S/(S+Q) and rescales, the same
+ *   partition of (0,1).)
+ * margin[t] = distance from T to the nearest bucket boundary / (S + Q); a
+ * token whose margin is below the FP32 rounding budget may legitimately come
+ * out differently on the GPU.  loglik_terms receives sum_t log(S+Q) and
+ * sum_t log(L_d + K*alpha) (the reference's per-token log term,
+ * lda_train_kernel.cu:258, summed in FP64 with Neumaier compensation).
+ */
+static inline void neumaier_add(double &sum, double &comp, double x) {
+    double t = sum + x;
+    if (std::fabs(sum) >= std::fabs(x))
+        comp += (sum - t) + x;
+    else
+        comp += (x - t) + sum;
+    sum = t;
+}
+
+void oracle_sample_fp64(int32_t num_docs, int32_t num_words, int32_t k, float alpha_f, float beta_f,
+                        const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr, const uint16_t *z,
+                        const int32_t *nk, const int16_t *theta_a, const int16_t *theta_ja, const int32_t *max_ia,
+                        const int32_t *cur_ia, uint64_t seed, uint32_t iteration, uint16_t *z_out, double *margin,
+                        double *loglik_terms) {
+    const double alpha = alpha_f, beta = beta_f;
+    const double vbeta = (double)num_words * beta;
+    std::vector<double> inv((size_t)k), ph((size_t)k);
+    std::vector<int32_t> hist((size_t)k);
+    for (int32_t j = 0; j < k; ++j) inv[j] = 1.0 / ((double)nk[j] + vbeta);
+    double s_log = 0, c_log = 0, s_doc = 0, c_doc = 0;
+    for (int32_t w = 0; w < num_words; ++w) {
+        std::fill(hist.begin(), hist.end(), 0);
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) hist[z[t]]++;
+        double q = 0;
+        for (int32_t j = 0; j < k; ++j) {
+            ph[j] = ((double)hist[j] + beta) / ((double)nk[j] + vbeta);
+            q += alpha * ph[j];
+        }
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) {
+            int32_t d = doc_ids[t];
+            int32_t rs = max_ia[d], re = cur_ia[d];
+            double s = 0;
+            for (int32_t i = rs; i < re; ++i)
+                if (theta_a[i] != 0) s += (double)(uint16_t)theta_a[i] * ph[(uint16_t)theta_ja[i]];
+            double total = s + q;
+            double u = oracle_uniform(philox_word0(seed, (uint64_t)t, iteration, 0u));
+            double target = u * total;
+            int32_t pick = -1;
+            double lo = 0, hi = total;
+            if (target < s) {
+                double cum = 0;
+                int32_t last = -1;
+                for (int32_t i = rs; i < re; ++i) {
+                    if (theta_a[i] == 0) continue;
+                    double nxt = cum + (double)(uint16_t)theta_a[i] * ph[(uint16_t)theta_ja[i]];
+                    last = i;
+                    if (nxt > target) {
+                        pick = (uint16_t)theta_ja[i];
+                        lo = cum;
+                        hi = nxt;
+                        break;
+                    }
+                    cum = nxt;
+                }
+                if (pick < 0) { /* cannot happen in exact arithmetic */
+                    pick = (uint16_t)theta_ja[last];
+                    lo = cum;
+                    hi = s;
+                }
+            } else {
+                double cum = s;
+                for (int32_t j = 0; j < k; ++j) {
+                    double nxt = cum + alpha * ph[j];
+                    if (nxt > target) {
+                        pick = j;
+                        lo = cum;
+                        hi = nxt;
+                        break;
+                    }
+                    cum = nxt;
+                }
+                if (pick < 0) {
+                    pick = k - 1;
+                    lo = cum;
+                    hi = total;
+                }
+            }
+            z_out[t] = (uint16_t)pick;
+            if (margin) margin[t] = std::min(target - lo, hi - target) / total;
+            int64_t len = doc_ptr[d + 1] - doc_ptr[d];
+            neumaier_add(s_log, c_log, std::log(total));
+            neumaier_add(s_doc, c_doc, std::log((double)len + (double)k * alpha));
+        }
+    }
+    if (loglik_terms) {
+        loglik_terms[0] = s_log + c_log;
+        loglik_terms[1] = s_doc + c_doc;
+    }
+}
+
+/* ------------------------------------------------------ joint likelihood */
+/*
+ * log p(w, z) = K lgamma(V b) - sum_k lgamma(n_k + V b) + sum_{w,k: n>0} [lgamma(n_wk + b) - lgamma(b)]
+ *             + D lgamma(K a) - sum_d lgamma(L_d + K a) + sum_{d,k: n>0} [lgamma(n_dk + a) - lgamma(a)]
+ * (collapsed LDA joint, Griffiths & Steyvers, PNAS 2004), FP64, Neumaier sums.
+ */
+double oracle_loglik_joint(int32_t num_docs, int32_t num_words, int32_t k, float alpha_f, float beta_f,
+                           const int64_t *word_ptr, const int64_t *doc_ptr, const int32_t *doc_tok, const uint16_t *z) {
+    const double a = alpha_f, b = beta_f, vb = (double)num_words * b, ka = (double)k * a;
+    const double lg_b = std::lgamma(b), lg_a = std::lgamma(a);
+    double s = 0, c = 0;
+    std::vector<int32_t> hist((size_t)k), nk((size_t)k, 0);
+    for (int32_t w = 0; w < num_words; ++w) {
+        std::fill(hist.begin(), hist.end(), 0);
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) hist[z[t]]++;
+        for (int32_t j = 0; j < k; ++j)
+            if (hist[j] > 0) {
+                neumaier_add(s, c, std::lgamma((double)hist[j] + b) - lg_b);
+                nk[j] += hist[j];
+            }
+    }
+    neumaier_add(s, c, (double)k * std::lgamma(vb));
+    for (int32_t j = 0; j < k; ++j) neumaier_add(s, c, -std::lgamma((double)nk[j] + vb));
+    neumaier_add(s, c, (double)num_docs * std::lgamma(ka));
+    for (int32_t d = 0; d < num_docs; ++d) {
+        std::fill(hist.begin(), hist.end(), 0);
+        for (int64_t i = doc_ptr[d]; i < doc_ptr[d + 1]; ++i) hist[z[doc_tok[i]]]++;
+        neumaier_add(s, c, -std::lgamma((double)(doc_ptr[d + 1] - doc_ptr[d]) + ka));
+        for (int32_t j = 0; j < k; ++j)
+            if (hist[j] > 0) neumaier_add(s, c, std::lgamma((double)hist[j] + a) - lg_a);
+    }
+    return s + c;
+}
+
+} /* extern "C" */

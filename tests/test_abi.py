@@ -1,0 +1,110 @@
+"""The C ABI surface: every declared entry point is exported, and the host-side
+checks run without a GPU."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import culda_cgs_b200 as cb
+from culda_cgs_b200 import _ffi
+from culda_cgs_b200.configs import TINY
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "culda_b200.h"
+
+
+def declared_functions() -> set[str]:
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return set(re.findall(r"\b(culda_\w+)\s*\(", text))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 25
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_ffi.library_path())], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert names <= exported, names - exported
+    assert {n for n in exported if n.startswith("culda_")} == names  # nothing else leaks
+    assert names == set(_ffi.SIGNATURES)
+
+
+def test_version_and_status_strings():
+    lib = cb.lib()
+    assert b"sm_100a" in lib.culda_version()
+    assert lib.culda_status_string(0) == b"ok"
+    assert lib.culda_status_string(-8) == b"no CUDA device"
+
+
+def _params(**kw):
+    d = dict(k=64, alpha=0.1, beta=0.01, seed=1, device=0, group_lanes=0, item_tokens=0, flags=0)
+    d.update(kw)
+    return _ffi.Params(**d)
+
+
+@pytest.mark.parametrize("kw", [dict(k=48), dict(k=0), dict(k=8192), dict(alpha=0.0), dict(beta=-1.0),
+                                dict(group_lanes=3)])
+def test_create_rejects_bad_params(kw):
+    c = cb.Corpus.generate(TINY.gen)
+    ctx = C.c_void_p()
+    p = _params(**kw)
+    assert cb.lib().culda_create(c.c_ptr, C.byref(p), C.byref(ctx)) == _ffi.CULDA_ERR_INVALID_ARG
+    assert not ctx.value
+
+
+def test_create_rejects_inconsistent_corpus():
+    c = cb.Corpus.generate(TINY.gen)
+    dp = c.doc_ptr.copy()
+    dp[-1] += 1
+    b = cb.Corpus.from_arrays(dp, c.word_ptr, c.doc_ids)
+    ctx = C.c_void_p()
+    assert cb.lib().culda_create(b.c_ptr, C.byref(_params()), C.byref(ctx)) == _ffi.CULDA_ERR_FORMAT
+
+
+def test_create_rejects_docs_over_16bit_counts():
+    n = 70000
+    b = cb.Corpus.from_arrays(np.array([0, n]), np.array([0, n]), np.zeros(n, dtype=np.int32))
+    ctx = C.c_void_p()
+    assert cb.lib().culda_create(b.c_ptr, C.byref(_params()), C.byref(ctx)) == _ffi.CULDA_ERR_UNSUPPORTED
+
+
+def test_create_without_device_fails_cleanly(has_gpu):
+    if has_gpu:
+        pytest.skip("a device is present")
+    c = cb.Corpus.generate(TINY.gen)
+    ctx = C.c_void_p()
+    assert cb.lib().culda_create(c.c_ptr, C.byref(_params()), C.byref(ctx)) == _ffi.CULDA_ERR_NO_DEVICE
+    assert b"no CUDA device" in cb.lib().culda_last_error(None)
+
+
+def build_items(word_ptr, item_tokens):
+    wp = np.ascontiguousarray(word_ptr, dtype=np.int64)
+    lib = cb.lib()
+    nhot = C.c_int32()
+    n = lib.culda_build_items(len(wp) - 1, wp.ctypes.data_as(C.POINTER(C.c_int64)), item_tokens, None, 0,
+                              C.byref(nhot))
+    items = (_ffi.Item * n)()
+    assert lib.culda_build_items(len(wp) - 1, wp.ctypes.data_as(C.POINTER(C.c_int64)), item_tokens, items, n,
+                                 C.byref(nhot)) == n
+    return [(it.begin, it.count, it.word, it.hot, it.first) for it in items], nhot.value
+
+
+def test_build_items_splits_hot_words_and_covers_every_token():
+    lens = np.array([5000, 0, 3, 2500, 2501, 1, 0, 7])
+    wp = np.concatenate([[0], np.cumsum(lens)])
+    items, nhot = build_items(wp, 2500)
+    assert nhot == 2
+    counts = [it[1] for it in items]
+    assert counts == sorted(counts, reverse=True) and max(counts) <= 2500
+    covered = np.zeros(wp[-1], dtype=int)
+    for b, n, w, hot, first in items:
+        assert wp[w] <= b and b + n <= wp[w + 1]
+        covered[b:b + n] += 1
+        assert (hot >= 0) == (lens[w] > 2500)
+    assert (covered == 1).all()
+    assert sum(it[4] for it in items) == int((lens > 0).sum())  # one first item per non-empty word

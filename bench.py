@@ -56,22 +56,34 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
         self._t = None
+        self.t0 = self.t1 = None
 
     def start(self):
+        """Starts sampling and returns once the first sample has arrived."""
         exe = shutil.which("nvidia-smi")
         if not exe:
             return
         self.proc = subprocess.Popen([exe, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                      "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                      "-lms", "50", "-i", str(self.device)], stdout=subprocess.PIPE,
                                      stderr=subprocess.DEVNULL, text=True)
         self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        deadline = time.time() + 10
+        while not self.lines and time.time() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(0.12)  # let the sample that covers the end arrive
 
     def stop(self) -> dict | None:
         if not self.proc:
@@ -83,9 +95,16 @@ class ClockSampler:
             self.proc.kill()
         if self._t:
             self._t.join(timeout=2)
+        lines = self.lines
+        if self.t0 is not None and self.t1 is not None:
+            inside = [x for x in lines if self.t0 <= x[0] <= self.t1 + 0.1]
+            if not inside:  # region shorter than the sampling period: nearest samples
+                mid = 0.5 * (self.t0 + self.t1)
+                inside = sorted(lines, key=lambda x: abs(x[0] - mid))[:2]
+            lines = inside
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for _, line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 8:
                 continue
@@ -193,14 +212,16 @@ def run_ours(args, world, rank, local, pg):
                item_tokens=args.item_tokens)
     info = m.info()
     log(f"[rank {rank}] info {info}")
+    clocks = ClockSampler(local)
+    clocks.start()
     warm = m.iterate(args.warmup) if args.warmup > 0 else []
     barrier(pg)
     cuda_sync()
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks.mark_start()
     stats = m.iterate(args.steps)
     cuda_sync()
     barrier(pg)
+    clocks.mark_end()
     clk = clocks.stop()
     dev_seconds = sum(s["seconds"] for s in stats)
     max_seconds = allreduce_max(pg, dev_seconds)
@@ -322,7 +343,7 @@ def run_reference(args, world, rank):
         clocks = ClockSampler(0)
         clocks.start()
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=args.ref_timeout)
-        clk = clocks.stop()
+        clk = clocks.stop()  # the whole run (load included): its iterations are not separable here
         rows = [m.groups() for m in ITER_RE.finditer(r.stdout)]
         if r.returncode != 0 or len(rows) < iters:
             tail = (r.stdout + r.stderr)[-400:].replace("\n", " | ")

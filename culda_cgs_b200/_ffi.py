@@ -25,7 +25,7 @@ CULDA_ERR_DEVICE_STATE = -7
 CULDA_ERR_NO_DEVICE = -8
 
 CULDA_LEN_POISSON, CULDA_LEN_LOGNORMAL, CULDA_LEN_PARETO = 0, 1, 2
-CULDA_FLAG_NO_GRAPH, CULDA_FLAG_VERBOSE = 1, 2
+CULDA_FLAG_NO_GRAPH, CULDA_FLAG_VERBOSE, CULDA_FLAG_NO_REORDER = 1, 2, 4
 
 
 class Corpus(C.Structure):
@@ -57,14 +57,17 @@ class Info(C.Structure):
 
 
 class Item(C.Structure):
-    _fields_ = [("begin", i64), ("count", i32), ("word", i32), ("hot", i32), ("first", i32)]
+    _fields_ = [("begin", i64), ("count", i32), ("word", i32), ("hot", i32), ("first", i32), ("seg_begin", i32),
+                ("seg_count", i32)]
 
 
 class SampleArgs(C.Structure):
     _fields_ = [("k", i32), ("alpha", f32), ("beta", f32), ("num_docs", i32), ("num_words", i32),
                 ("num_tokens", i64), ("word_ptr", C.c_void_p), ("doc_ids", C.c_void_p), ("topics_in", C.c_void_p),
                 ("topics_out", C.c_void_p), ("theta", C.c_void_p), ("theta_rows", C.c_void_p), ("nk", C.c_void_p),
-                ("items", C.c_void_p), ("num_items", i32), ("num_hot", i32), ("hot_items", C.c_void_p),
+                ("items", C.c_void_p), ("seg_start", C.c_void_p), ("num_segs", i32), ("num_items", i32),
+                ("num_hot", i32),
+                ("hot_items", C.c_void_p),
                 ("num_hot_items", i32), ("theta_capacity", i64), ("seed", u64), ("iteration", u32),
                 ("group_lanes", i32), ("loglik_sum", C.c_void_p), ("error", C.c_void_p)]
 
@@ -93,6 +96,7 @@ SIGNATURES = {
     "culda_last_error": (C.c_char_p, [C.c_void_p]),
     "culda_destroy": (None, [C.c_void_p]),
     "culda_build_items": (i64, [i32, P(i64), i32, P(Item), i64, P(i32)]),
+    "culda_build_segments": (i64, [i64, P(i32), P(Item), i32, i32, P(i32), i64]),
     "culda_update_phi": (C.c_int, [i32, i32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "culda_compute_phi_head": (C.c_int, [i32, f32, i32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "culda_update_theta_workspace": (C.c_size_t, [i32, i32]),

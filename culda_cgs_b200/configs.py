@@ -37,6 +37,12 @@ SCALE = Workload("plain-cgs-scale V=100k D=300k N~60M K=1024",
                  GenConfig(num_words=100_000, num_topics=500, num_docs=300_000, len_law=CULDA_LEN_LOGNORMAL,
                            len_a=5.0, len_b=0.8, len_min=5, len_max=5000), iterations=100)
 
+# ~12M tokens, the same generator as SCALE with a fifth of the docs: inputs
+# still above the L2 size, small enough for detailed profiler captures.
+MEDIUM = Workload("plain-cgs-medium V=100k D=60k N~12M K=1024",
+                  GenConfig(num_words=100_000, num_topics=500, num_docs=60_000, len_law=CULDA_LEN_LOGNORMAL,
+                            len_a=5.0, len_b=0.8, len_min=5, len_max=5000), iterations=100)
+
 # ~100M tokens of very uneven documents: V=1M Zipf(1.1), 1000 generating
 # topics, 2M docs with Pareto(1.5, 20) lengths clipped at 50k.
 UNEVEN = Workload("batched-uneven V=1M D=2M N~100M",
@@ -52,4 +58,4 @@ MINI = Workload("mini V=3k D=2k K=1024",
                 GenConfig(num_words=3_000, num_topics=40, num_docs=2_000, len_law=CULDA_LEN_LOGNORMAL, len_a=4.0,
                           len_b=0.8, len_min=1, len_max=1500), k=1024, iterations=5)
 
-WORKLOADS = {w.name.split()[0]: w for w in (SMALL, SCALE, UNEVEN, TINY, MINI)}
+WORKLOADS = {w.name.split()[0]: w for w in (SMALL, SCALE, MEDIUM, UNEVEN, TINY, MINI)}

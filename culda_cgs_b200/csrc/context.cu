@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -37,15 +38,22 @@ struct culda_ctx {
     int item_tokens = 0;
 
     int64_t *d_word_ptr = nullptr, *d_doc_ptr = nullptr;
-    int32_t *d_doc_ids = nullptr, *d_doc_tok = nullptr, *d_doc_order = nullptr;
+    // Tokens are stored word by word as in the input, but inside each word
+    // ordered by their doc's length; d_tok_index[i] is the input (word-major)
+    // index of stored token i, the key of its Philox stream and of copy-out.
+    int32_t *d_doc_ids = nullptr, *d_doc_tok = nullptr, *d_doc_order = nullptr, *d_tok_index = nullptr;
     uint16_t *d_z[2] = {nullptr, nullptr};
+    uint16_t *d_zx = nullptr;  // topics in input order for copy-in / copy-out
+    float *d_u = nullptr;      // the tokens' uniforms of the current iteration
     int cur = 0;
-    uint32_t *d_theta = nullptr;
+    ThetaEntry *d_theta = nullptr;
     int64_t theta_cap = 0;
     int2 *d_rows = nullptr;
     int32_t *d_nk = nullptr;
     culda_item *d_items = nullptr, *d_hot_items = nullptr;
     int32_t num_items = 0, num_hot_items = 0, num_hot = 0;
+    int32_t *d_seg_start = nullptr;  // first stored token of every segment
+    int32_t num_segs = 0;
     int32_t *d_hot_phi = nullptr;
     double *d_item_ll = nullptr;
     int32_t *d_counter = nullptr;
@@ -92,24 +100,12 @@ cudaError_t dalloc(T **p, size_t n) {
     return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
 }
 
-__global__ void iota_kernel(int64_t n, int32_t *v) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v[i] = (int32_t)i;
-}
-
-__global__ void copy_error_kernel(const int32_t *err, DevStats *st) { st->error = *err; }
-
-int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
-    const int nxt = 1 - cur;
-    CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
-    if (ctx->num_hot > 0) {
-        CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
-        CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
-                           s));
-    }
-    CK(cudaEventRecord(ctx->ev_s0, s));
+// Sampler parameters for topics d_z[cur] -> d_z[1-cur]; the Philox iteration
+// comes from the device counter when iteration_ptr is set (graph launches).
+SampleParams sample_params(const culda_ctx *ctx, int cur, uint32_t iteration, const uint32_t *iteration_ptr) {
     SampleParams p{};
     p.k = ctx->K;
+    p.kmask = pow2_ceil(ctx->K) - 1;
     p.alpha = ctx->params.alpha;
     p.beta = ctx->params.beta;
     p.vbeta = ctx->params.beta * (float)ctx->V;
@@ -119,29 +115,59 @@ int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
     p.num_tokens = ctx->N;
     p.theta_cap = ctx->theta_cap;
     p.doc_ids = ctx->d_doc_ids;
+    p.tok_index = ctx->d_tok_index;
+    p.uniforms = ctx->d_u;
     p.topics_in = ctx->d_z[cur];
-    p.topics_out = ctx->d_z[nxt];
+    p.topics_out = ctx->d_z[1 - cur];
     p.theta = ctx->d_theta;
     p.rows = ctx->d_rows;
     p.nk = ctx->d_nk;
     p.items = ctx->d_items;
+    p.seg_start = ctx->d_seg_start;
+    p.num_segs = ctx->num_segs;
     p.hot_phi = ctx->d_hot_phi;
     p.item_counter = ctx->d_counter;
     p.item_ll = ctx->d_item_ll;
     p.seed = ctx->params.seed;
-    p.iteration = 0;
-    p.iteration_ptr = ctx->d_iter;
+    p.iteration = iteration;
+    p.iteration_ptr = iteration_ptr;
     p.error = ctx->d_error;
-    CK(launch_sample(p, ctx->group_lanes, ctx->sample_grid, s));
-    CK(cudaEventRecord(ctx->ev_s1, s));
+    return p;
+}
+
+__global__ void copy_error_kernel(const int32_t *err, DevStats *st) { st->error = *err; }
+
+// Inside a stream capture a plain event record only orders the capture; the
+// external flag turns it into an event-record node of the graph so the event
+// can be timed after each launch.
+cudaError_t record_event(cudaEvent_t ev, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cs);
+    if (e != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal)
+                                               : cudaEventRecord(ev, s);
+}
+
+int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
+    const int nxt = 1 - cur;
+    CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
+    if (ctx->num_hot > 0) {
+        CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
+        CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
+                           s));
+    }
+    CK(launch_uniforms(ctx->N, ctx->params.seed, ctx->d_iter, 0u, ctx->d_tok_index, ctx->d_u, s));
+    CK(record_event(ctx->ev_s0, s));
+    CK(launch_sample(sample_params(ctx, cur, 0u, ctx->d_iter), ctx->group_lanes, ctx->sample_grid, s));
+    CK(record_event(ctx->ev_s1, s));
     CK(launch_finalize_ll(ctx->d_item_ll, ctx->num_items, ctx->d_stats, ctx->d_iter, s));
     CK(cudaMemsetAsync(ctx->d_nk, 0, sizeof(int32_t) * (size_t)ctx->K, s));
     CK(cudaMemsetAsync(&ctx->d_stats->row_entries, 0, 3 * sizeof(int64_t), s));
-    CK(cudaEventRecord(ctx->ev_t0, s));
+    CK(record_event(ctx->ev_t0, s));
     CK(launch_theta_rebuild(ctx->K, ctx->D, ctx->d_doc_ptr, ctx->d_doc_tok, ctx->d_z[nxt], ctx->d_doc_order,
                             ctx->d_rows, ctx->d_theta, ctx->d_nk, &ctx->d_stats->row_entries, ctx->d_error,
                             ctx->theta_grid, s));
-    CK(cudaEventRecord(ctx->ev_t1, s));
+    CK(record_event(ctx->ev_t1, s));
     copy_error_kernel<<<1, 1, 0, s>>>(ctx->d_error, ctx->d_stats);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, s));
@@ -230,6 +256,135 @@ extern "C" int64_t culda_build_items(int32_t num_words, const int64_t *word_ptr,
     }
     return (int64_t)v.size();
 }
+
+extern "C" int64_t culda_build_segments(int64_t num_tokens, const int32_t *doc_ids, culda_item *items,
+                                        int32_t num_items, int32_t max_len, int32_t *seg_start, int64_t max_segs) {
+    if (num_tokens <= 0 || !doc_ids || !items || num_items <= 0 || max_len <= 0) {
+        set_global_error("culda_build_segments: invalid argument");
+        return CULDA_ERR_INVALID_ARG;
+    }
+    int64_t n = 0;
+    for (int32_t i = 0; i < num_items; ++i) {
+        culda_item &it = items[i];
+        if (it.begin < 0 || it.count <= 0 || it.begin + it.count > num_tokens) {
+            set_global_error("culda_build_segments: item %d outside the token range", i);
+            return CULDA_ERR_INVALID_ARG;
+        }
+        const int64_t first = n;
+        int64_t len = 0;
+        for (int64_t t = it.begin; t < it.begin + it.count; ++t) {
+            if (t == it.begin || doc_ids[t] != doc_ids[t - 1] || len == max_len) {
+                if (seg_start) {
+                    if (n >= max_segs) {
+                        set_global_error("culda_build_segments: more than %lld segments", (long long)max_segs);
+                        return CULDA_ERR_INVALID_ARG;
+                    }
+                    seg_start[n] = (int32_t)t;
+                }
+                ++n;
+                len = 0;
+            }
+            ++len;
+        }
+        if (n >= INT32_MAX) return CULDA_ERR_UNSUPPORTED;
+        it.seg_begin = (int32_t)first;
+        it.seg_count = (int32_t)(n - first);
+    }
+    return n;
+}
+
+namespace {
+
+constexpr int kSegmentMax = 32;  // tokens per segment (bounds the work of one group on one row)
+
+__global__ void mark_items_kernel(const culda_item *__restrict__ items, int num_items, int32_t *mark) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_items; i += gridDim.x * blockDim.x)
+        mark[items[i].begin] = 1;
+}
+
+// key[t] = t where a run of one doc starts (item start or doc change), else 0
+__global__ void run_key_kernel(int64_t n, const int32_t *__restrict__ doc_ids, const int32_t *__restrict__ mark,
+                               int32_t *key) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        key[t] = (t == 0 || mark[t] || doc_ids[t] != doc_ids[t - 1]) ? (int32_t)t : 0;
+}
+
+struct MaxOp {
+    __device__ __forceinline__ int32_t operator()(int32_t a, int32_t b) const { return a > b ? a : b; }
+};
+
+// flag[t] = 1 where a segment starts: every max_len tokens from a run start
+__global__ void seg_flag_kernel(int64_t n, const int32_t *__restrict__ run_start, int32_t *flag) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= n; t += (int64_t)gridDim.x * blockDim.x)
+        flag[t] = t < n && ((t - run_start[t]) % kSegmentMax) == 0 ? 1 : 0;
+}
+
+__global__ void seg_scatter_kernel(int64_t n, const int32_t *__restrict__ flag, const int32_t *__restrict__ index,
+                                   int32_t *seg_start) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        if (flag[t]) seg_start[index[t]] = (int32_t)t;
+}
+
+__global__ void item_segments_kernel(culda_item *items, int num_items, const int32_t *__restrict__ index) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_items; i += gridDim.x * blockDim.x) {
+        culda_item &it = items[i];
+        it.seg_begin = index[it.begin];
+        it.seg_count = index[it.begin + it.count] - it.seg_begin;
+    }
+}
+
+// Segments of the stored token order, on the device (see culda_build_segments).
+int build_segments_device(culda_ctx *ctx) {
+    cudaStream_t s = ctx->stream;
+    const int64_t N = ctx->N;
+    int32_t *mark = nullptr, *key = nullptr, *run = nullptr, *flag = nullptr, *index = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0, b2 = 0;
+    int rc = CULDA_OK;
+    auto grid = [](int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); };
+    do {
+#define CKS(call)                                                                                          \
+    {                                                                                                      \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) {                                                                           \
+            rc = fail(ctx, CULDA_ERR_CUDA, "segments: %s: %s", #call, cudaGetErrorString(e_));             \
+            break;                                                                                         \
+        }                                                                                                  \
+    }
+        CKS(dalloc(&mark, (size_t)N));
+        CKS(dalloc(&key, (size_t)N));
+        CKS(dalloc(&run, (size_t)N));
+        CKS(dalloc(&flag, (size_t)N + 1));
+        CKS(dalloc(&index, (size_t)N + 1));
+        CKS(cudaMemsetAsync(mark, 0, sizeof(int32_t) * (size_t)N, s));
+        mark_items_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, mark);
+        run_key_kernel<<<grid(N), 256, 0, s>>>(N, ctx->d_doc_ids, mark, key);
+        CKS(cudaGetLastError());
+        CKS(cub::DeviceScan::InclusiveScan(nullptr, tmp_bytes, key, run, MaxOp(), (int)N, s));
+        CKS(cub::DeviceScan::ExclusiveSum(nullptr, b2, flag, index, (int)N + 1, s));
+        tmp_bytes = std::max(tmp_bytes, b2);
+        CKS(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 1)));
+        CKS(cub::DeviceScan::InclusiveScan(tmp, tmp_bytes, key, run, MaxOp(), (int)N, s));
+        seg_flag_kernel<<<grid(N + 1), 256, 0, s>>>(N, run, flag);
+        CKS(cudaGetLastError());
+        CKS(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, flag, index, (int)N + 1, s));
+        int32_t total = 0;
+        CKS(cudaMemcpyAsync(&total, index + N, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CKS(cudaStreamSynchronize(s));
+        ctx->num_segs = total;
+        CKS(dalloc(&ctx->d_seg_start, (size_t)total));
+        seg_scatter_kernel<<<grid(N), 256, 0, s>>>(N, flag, index, ctx->d_seg_start);
+        item_segments_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, index);
+        CKS(cudaGetLastError());
+        CKS(cudaStreamSynchronize(s));
+#undef CKS
+    } while (0);
+    for (void *b : {(void *)mark, (void *)key, (void *)run, (void *)flag, (void *)index, tmp})
+        if (b) cudaFree(b);
+    return rc;
+}
+
+}  // namespace
 
 // --------------------------------------------------------------- create
 extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_ctx **out) {
@@ -336,15 +491,48 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
             }
     }
 
-    // doc-reverse index: stable radix sort of token ids by doc id
+    // Stored token order: inside each word, tokens sorted by their doc's
+    // length, longest first (a stable sort on (word, 65535 - L_d) keeps doc
+    // order among equal lengths).  Neighbouring sampler groups then walk theta
+    // rows of similar length.  Sampling results do not depend on this order:
+    // each token's Philox stream is keyed on its input index.
+    if (!(p->flags & CULDA_FLAG_NO_REORDER)) {
+        uint64_t *keys = nullptr, *keys_out = nullptr;
+        int32_t *vals = nullptr, *ids2 = nullptr;
+        CKB(dalloc(&keys, (size_t)N));
+        CKB(dalloc(&keys_out, (size_t)N));
+        CKB(dalloc(&vals, (size_t)N));
+        CKB(dalloc(&ctx->d_tok_index, (size_t)N));
+        CKB(launch_order_keys(V, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, keys, s));
+        CKB(launch_iota(N, vals, s));
+        int end_bit = 17;
+        while ((1ll << (end_bit - 16)) < (int64_t)V) ++end_bit;
+        size_t tmp_bytes = 0;
+        CKB(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
+                                            end_bit, s));
+        void *tmp = nullptr;
+        CKB(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 1)));
+        CKB(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
+                                            end_bit, s));
+        CKB(dalloc(&ids2, (size_t)N));
+        CKB(launch_gather<int32_t>(N, ctx->d_tok_index, ctx->d_doc_ids, ids2, s));
+        CKB(cudaStreamSynchronize(s));
+        cudaFree(tmp);
+        cudaFree(keys);
+        cudaFree(keys_out);
+        cudaFree(vals);
+        cudaFree(ctx->d_doc_ids);
+        ctx->d_doc_ids = ids2;
+    }
+
+    // doc-reverse index: stable radix sort of stored token positions by doc id
     // (the reference builds it on the host, doc_chunk.cpp:225-255)
     {
         CKB(dalloc(&ctx->d_doc_tok, (size_t)N));
         int32_t *keys_out = nullptr, *vals_in = nullptr;
         CKB(dalloc(&keys_out, (size_t)N));
         CKB(dalloc(&vals_in, (size_t)N));
-        iota_kernel<<<1024, 256, 0, s>>>(N, vals_in);
-        CKB(cudaGetLastError());
+        CKB(launch_iota(N, vals_in, s));
         int end_bit = 1;
         while ((1ll << end_bit) < (int64_t)D) ++end_bit;
         size_t tmp_bytes = 0;
@@ -382,7 +570,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     ctx->h_max_ia[D] = (int32_t)off;
     ctx->theta_cap = off;
     CKB(dalloc(&ctx->d_theta, (size_t)off));
-    CKB(cudaMemsetAsync(ctx->d_theta, 0, sizeof(uint32_t) * (size_t)std::max<int64_t>(off, 1), s));
+    CKB(cudaMemsetAsync(ctx->d_theta, 0, sizeof(ThetaEntry) * (size_t)std::max<int64_t>(off, 1), s));
     CKB(dalloc(&ctx->d_rows, (size_t)D));
     CKB(cudaMemcpyAsync(ctx->d_rows, rows.data(), sizeof(int2) * (size_t)D, cudaMemcpyHostToDevice, s));
 
@@ -438,6 +626,8 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         CKB(cudaStreamSynchronize(s));
     }
     ctx->sample_grid = std::max(1, std::min(ctx->num_items, sms * sbps));
+    rc = build_segments_device(ctx);
+    if (rc) return bail(rc);
 
     CKB(dalloc(&ctx->d_counter, 64));
     CKB(dalloc(&ctx->d_iter, 1));
@@ -452,7 +642,9 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     // topics: Philox init, then the initial counts (SingleChunkSingleGPU.h:24-41)
     CKB(dalloc(&ctx->d_z[0], (size_t)N));
     CKB(dalloc(&ctx->d_z[1], (size_t)N));
-    CKB(launch_init_topics(N, K, p->seed, ctx->d_z[0], s));
+    CKB(dalloc(&ctx->d_zx, (size_t)N));
+    CKB(dalloc(&ctx->d_u, (size_t)N));
+    CKB(launch_init_topics(N, K, p->seed, ctx->d_tok_index, ctx->d_z[0], s));
     ctx->cur = 0;
     rc = rebuild_counts(ctx);
     if (rc) return bail(rc);
@@ -508,23 +700,42 @@ extern "C" int culda_iterate(culda_ctx *ctx, int n, culda_iter_stats *stats) {
     return CULDA_OK;
 }
 
+// Device topics in stored order -> host array in input (word-major) order.
+static int topics_to_host(culda_ctx *ctx, const uint16_t *d_src, uint16_t *host) {
+    cudaStream_t s = ctx->stream;
+    if (ctx->d_tok_index) {
+        CK(launch_scatter<uint16_t>(ctx->N, ctx->d_tok_index, d_src, ctx->d_zx, s));
+        d_src = ctx->d_zx;
+    }
+    CK(cudaMemcpyAsync(host, d_src, sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return CULDA_OK;
+}
+
 extern "C" int culda_set_topics(culda_ctx *ctx, const uint16_t *topics) {
     if (!ctx || !topics) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_set_topics: null argument");
     CK(cudaSetDevice(ctx->device));
-    CK(cudaMemcpyAsync(ctx->d_z[ctx->cur], topics, sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyHostToDevice,
-                       ctx->stream));
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_zx, topics, sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyHostToDevice, s));
+    int32_t *flag = ctx->d_error + 32;  // a spare word of the error buffer
+    CK(cudaMemsetAsync(flag, 0, sizeof(int32_t), s));
+    CK(launch_check_topics(ctx->N, ctx->K, ctx->d_zx, flag, s));
+    int32_t bad = 0;
+    CK(cudaMemcpyAsync(&bad, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (bad) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_set_topics: a topic is >= K=%d; state unchanged", ctx->K);
+    if (ctx->d_tok_index)
+        CK(launch_gather<uint16_t>(ctx->N, ctx->d_tok_index, ctx->d_zx, ctx->d_z[ctx->cur], s));
+    else
+        CK(cudaMemcpyAsync(ctx->d_z[ctx->cur], ctx->d_zx, sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyDeviceToDevice,
+                           s));
     return rebuild_counts(ctx);
 }
 
 extern "C" int culda_get_topics(culda_ctx *ctx, uint16_t *topics) {
     if (!ctx) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_get_topics: null context");
     CK(cudaSetDevice(ctx->device));
-    if (topics) {
-        CK(cudaMemcpyAsync(topics, ctx->d_z[ctx->cur], sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyDeviceToHost,
-                           ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-    }
-    return CULDA_OK;
+    return topics ? topics_to_host(ctx, ctx->d_z[ctx->cur], topics) : CULDA_OK;
 }
 
 extern "C" int culda_get_phi(culda_ctx *ctx, int32_t *phi, int32_t *nk) {
@@ -555,12 +766,15 @@ extern "C" int culda_get_theta(culda_ctx *ctx, int16_t *theta_a, int16_t *theta_
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     if (theta_a || theta_ja) {
-        std::vector<uint32_t> t((size_t)ctx->theta_cap);
-        CK(cudaMemcpyAsync(t.data(), ctx->d_theta, sizeof(uint32_t) * t.size(), cudaMemcpyDeviceToHost, s));
+        std::vector<ThetaEntry> t((size_t)ctx->theta_cap);
+        CK(cudaMemcpyAsync(t.data(), ctx->d_theta, sizeof(ThetaEntry) * t.size(), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         for (size_t i = 0; i < t.size(); ++i) {
-            if (theta_a) theta_a[i] = (int16_t)(uint16_t)(t[i] >> 16);
-            if (theta_ja) theta_ja[i] = (int16_t)(uint16_t)(t[i] & 0xFFFFu);
+            float cnt;
+            std::memcpy(&cnt, &t[i].x, sizeof(float));
+            // the reference stores counts as int16 (thetaA): same truncation
+            if (theta_a) theta_a[i] = (int16_t)(uint16_t)(uint32_t)cnt;
+            if (theta_ja) theta_ja[i] = (int16_t)(uint16_t)(t[i].y >> 2);  // stored as 4 * topic
         }
     }
     if (max_ia) std::copy(ctx->h_max_ia.begin(), ctx->h_max_ia.end(), max_ia);
@@ -587,42 +801,17 @@ extern "C" int culda_sample_snapshot(culda_ctx *ctx, uint32_t iteration, uint16_
         CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
                            s));
     }
-    SampleParams p{};
-    p.k = ctx->K;
-    p.alpha = ctx->params.alpha;
-    p.beta = ctx->params.beta;
-    p.vbeta = ctx->params.beta * (float)ctx->V;
-    p.num_docs = ctx->D;
-    p.num_items = ctx->num_items;
-    p.num_hot = ctx->num_hot;
-    p.num_tokens = ctx->N;
-    p.theta_cap = ctx->theta_cap;
-    p.doc_ids = ctx->d_doc_ids;
-    p.topics_in = ctx->d_z[cur];
-    p.topics_out = ctx->d_z[nxt];
-    p.theta = ctx->d_theta;
-    p.rows = ctx->d_rows;
-    p.nk = ctx->d_nk;
-    p.items = ctx->d_items;
-    p.hot_phi = ctx->d_hot_phi;
-    p.item_counter = ctx->d_counter;
-    p.item_ll = ctx->d_item_ll;
-    p.seed = ctx->params.seed;
-    p.iteration = iteration;
-    p.iteration_ptr = nullptr;
-    p.error = ctx->d_error;
-    CK(launch_sample(p, ctx->group_lanes, ctx->sample_grid, s));
+    CK(launch_uniforms(ctx->N, ctx->params.seed, nullptr, iteration, ctx->d_tok_index, ctx->d_u, s));
+    CK(launch_sample(sample_params(ctx, cur, iteration, nullptr), ctx->group_lanes, ctx->sample_grid, s));
     CK(launch_finalize_ll(ctx->d_item_ll, ctx->num_items, ctx->d_stats, nullptr, s));
     DevStats h{};
     int32_t e = 0;
     CK(cudaMemcpyAsync(&h, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    if (topics_out)
-        CK(cudaMemcpyAsync(topics_out, ctx->d_z[nxt], sizeof(uint16_t) * (size_t)ctx->N, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (loglik) *loglik = (h.ll_sum - ctx->doc_term) / (double)ctx->N;
     if (e) return fail(ctx, CULDA_ERR_DEVICE_STATE, "sampler reported device error 0x%x", e);
-    return CULDA_OK;
+    return topics_out ? topics_to_host(ctx, ctx->d_z[nxt], topics_out) : CULDA_OK;
 }
 
 extern "C" int culda_loglik_joint(culda_ctx *ctx, double *ll) {
@@ -633,8 +822,8 @@ extern "C" int culda_loglik_joint(culda_ctx *ctx, double *ll) {
     double *d_part = nullptr;
     CK(dalloc(&d_part, (size_t)P));
     CK(launch_loglik_joint(ctx->K, ctx->V, ctx->D, ctx->params.alpha, ctx->params.beta, ctx->d_word_ptr,
-                           ctx->d_z[ctx->cur], ctx->d_rows, ctx->d_theta, ctx->d_doc_ptr, ctx->d_nk, d_part, P,
-                           ctx->d_error, s));
+                           ctx->d_z[ctx->cur], ctx->d_rows, ctx->d_theta, ctx->d_doc_ptr, d_part, P, ctx->d_error,
+                           s));
     std::vector<double> part((size_t)P);
     std::vector<int32_t> nk((size_t)ctx->K);
     CK(cudaMemcpyAsync(part.data(), d_part, sizeof(double) * (size_t)P, cudaMemcpyDeviceToHost, s));
@@ -668,13 +857,14 @@ extern "C" int culda_get_info(const culda_ctx *ctx, culda_info *info) {
     info->group_lanes = ctx->group_lanes;
     info->sample_grid = ctx->sample_grid;
     info->theta_grid = ctx->theta_grid;
-    // hot_rows (when words are split), sample, finalize_ll, theta_rebuild, copy_error
-    info->kernels_per_iteration = (ctx->num_hot > 0 ? 1 : 0) + 4;
+    // hot_rows (when words are split), uniforms, sample, finalize_ll, theta_rebuild, copy_error
+    info->kernels_per_iteration = (ctx->num_hot > 0 ? 1 : 0) + 5;
     info->theta_capacity = ctx->theta_cap;
     const int64_t N = ctx->N, D = ctx->D, V = ctx->V, K = ctx->K;
     info->device_bytes = 8 * (V + 1) + 8 * (D + 1) + 4 * N /*doc ids*/ + 4 * N /*doc_tok*/ + 4 * D /*order*/ +
-                         2 * 2 * N /*topics*/ + 4 * ctx->theta_cap + 8 * D /*rows*/ + 4 * K +
-                         (int64_t)sizeof(culda_item) * (ctx->num_items + ctx->num_hot_items) +
+                         (ctx->d_tok_index ? 4 * N : 0) + 3 * 2 * N /*topics x2 + copy buffer*/ + 4 * N /*uniforms*/ +
+                         (int64_t)sizeof(ThetaEntry) * ctx->theta_cap + 8 * D /*rows*/ + 4 * K +
+                         (int64_t)sizeof(culda_item) * (ctx->num_items + ctx->num_hot_items) + 4 * ctx->num_segs +
                          4 * (int64_t)ctx->num_hot * K + 8 * (int64_t)ctx->num_items;
     info->doc_term = ctx->doc_term;
     return CULDA_OK;
@@ -689,8 +879,10 @@ extern "C" void culda_destroy(culda_ctx *ctx) {
     for (int c = 0; c < 2; ++c)
         if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
     void *bufs[] = {ctx->d_word_ptr, ctx->d_doc_ptr, ctx->d_doc_ids,  ctx->d_doc_tok,  ctx->d_doc_order,
+                    ctx->d_tok_index, ctx->d_zx,     ctx->d_u,
                     ctx->d_z[0],     ctx->d_z[1],    ctx->d_theta,    ctx->d_rows,     ctx->d_nk,
                     ctx->d_items,    ctx->d_hot_items, ctx->d_hot_phi, ctx->d_item_ll, ctx->d_counter,
+                    ctx->d_seg_start,
                     ctx->d_iter,     ctx->d_stats,   ctx->d_error};
     for (void *b : bufs)
         if (b) cudaFree(b);

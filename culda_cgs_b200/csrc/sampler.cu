@@ -1,0 +1,539 @@
+// sampler.cu — the sm_100a sampling kernel of the one-GPU CGS iteration
+// (replaces LDAKernelTrain, src_culda/kernel/lda_train_kernel.cu:20-271).
+//
+// Persistent CTAs pull work items (one word, or a slice of a hot word).  Per
+// item the word's phi row is built as a shared-memory histogram of the
+// snapshot topics (no dense V x K phi in HBM), phihat = (n_wk + beta) /
+// (n_k + V beta) is formed in FP32 at shared-memory offset 0, and the
+// alpha*phihat prefix of the dense bucket is scanned.  The item's tokens come
+// in segments (runs of one doc, at most 32 tokens): a group of G lanes walks
+// the doc's theta row once per segment with 32-byte loads (4 entries per lane
+// per step), keeping the running sum after every step in shared memory, and
+// then draws each token of the segment with its own Philox uniform.
+//
+// Theta entries are {float bits of the count, 4 * topic}: the product
+// theta_dk * phihat_wk is one shared-memory load at the entry's byte offset
+// and one multiply.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "device_util.cuh"
+#include "kernels.cuh"
+#include "philox.h"
+
+namespace culda {
+
+// theta_dk * phihat_wk for one entry.  The explicit-rounding intrinsics keep
+// the compiler from fusing products and sums into different FMAs in the two
+// passes: both passes must produce bitwise the same sums.
+__device__ __forceinline__ float entry_prob(uint32_t count_bits, uint32_t byte_off, const float *ph) {
+    return __fmul_rn(__uint_as_float(count_bits), *reinterpret_cast<const float *>(
+                                                       reinterpret_cast<const char *>(ph) + byte_off));
+}
+
+__device__ __forceinline__ float fsum(float a, float b) { return __fadd_rn(a, b); }
+
+// ------------------------------------------------------------ dense bucket
+// Inclusive prefix qc[j] = alpha * sum_{i<=j} ph[i].  Each thread owns a run of
+// ceil(K/T) entries summed with Neumaier compensation; the run totals are
+// scanned with Kogge-Stone shuffles, so every prefix carries an error of
+// about ten FP32 roundings.
+__device__ void dense_bucket_prefix(const float *ph, float *qc, int K, float alpha, float *s_warp) {
+    const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
+    const int per = (K + T - 1) / T;
+    const int b = min(tid * per, K), e = min(b + per, K);
+    float s = 0.f, c = 0.f;
+    for (int j = b; j < e; ++j) {
+        neumaier(s, c, alpha * ph[j]);
+        qc[j] = s + c;
+    }
+    const float tot = s + c;
+    float incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    float ex = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) ex = 0.f;
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        float w = lane < nwarps ? s_warp[lane] : 0.f;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        float wex = __shfl_up_sync(0xffffffffu, w, 1);
+        if (lane == 0) wex = 0.f;
+        if (lane < nwarps) s_warp[lane] = wex;
+    }
+    __syncthreads();
+    const float base = s_warp[warp] + ex;
+    for (int j = b; j < e; ++j) qc[j] = base + qc[j];
+}
+
+// First topic whose dense-bucket prefix exceeds tq (K-1 when none does).
+template <int G>
+__device__ __forceinline__ int dense_bucket_search(const float *qc, int K, float tq, int gl, unsigned m, int lane) {
+    if constexpr (G == 1) {
+        int lo = 0, hi = K - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (qc[mid] > tq)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        return lo;
+    } else {
+        int lo = 0, size = K;
+        while (size > 1) {
+            const int step = (size + G - 1) / G;
+            const int off = gl * step;
+            const int nseg = (size + step - 1) / step;
+            bool hit = false;
+            if (off < size) hit = qc[lo + min(off + step, size) - 1] > tq;
+            const unsigned b = group_ballot<G>(hit, m, lane);
+            const int j = b ? (__ffs(b) - 1) : (nseg - 1);
+            lo += j * step;
+            size = min(step, size - j * step);
+        }
+        return lo;
+    }
+}
+
+// ------------------------------------------------------------- row walk
+// Theta entries per lane per step (8 bytes each, loaded 16 bytes at a time).
+// Four keeps the sampler under 64 registers; eight needs about 80 and loses
+// occupancy for no gain on the 60M-token workload.
+constexpr int kLaneEntries = 4;
+constexpr int kLaneVecs = kLaneEntries / 2;
+
+template <int G>
+struct SampleShape {
+    static constexpr int kGroups = kSampleThreads / G;
+    static constexpr int kStep = kLaneEntries * G;          // entries per group step
+    static constexpr int kMaxSteps = 8 * G;                  // running sums kept per group
+    static constexpr int kPrefixFloats = kGroups * kMaxSteps;  // 1024 floats for every G
+};
+
+struct Step {
+    uint4 v[kLaneVecs];  // v[j] = {count 2j, offset 2j, count 2j+1, offset 2j+1}
+};
+
+__device__ __forceinline__ Step load_step(const ThetaEntry *__restrict__ theta, int idx, int re) {
+    Step st;
+    if (idx < re) {  // rows end on a multiple of 32 entries, idx on a multiple of kLaneEntries
+        const uint4 *p = reinterpret_cast<const uint4 *>(theta + idx);
+#pragma unroll
+        for (int j = 0; j < kLaneVecs; ++j) st.v[j] = __ldg(p + j);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kLaneVecs; ++j) st.v[j] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    return st;
+}
+
+__device__ __forceinline__ void step_probs(const Step &st, const float *ph, float p[kLaneEntries]) {
+#pragma unroll
+    for (int j = 0; j < kLaneVecs; ++j) {
+        p[2 * j] = entry_prob(st.v[j].x, st.v[j].y, ph);
+        p[2 * j + 1] = entry_prob(st.v[j].z, st.v[j].w, ph);
+    }
+}
+
+// Pairwise sum of the lane's entries.
+__device__ __forceinline__ float lane_sum(const float p[kLaneEntries]) {
+    float q[kLaneEntries];
+#pragma unroll
+    for (int i = 0; i < kLaneEntries; ++i) q[i] = p[i];
+#pragma unroll
+    for (int w = kLaneEntries / 2; w > 0; w >>= 1)
+#pragma unroll
+        for (int i = 0; i < w; ++i) q[i] = fsum(q[2 * i], q[2 * i + 1]);
+    return q[0];
+}
+
+// The group's last non-zero entry of a step (-1 when the step is all padding).
+template <int G>
+__device__ __forceinline__ int step_last_nonzero(const Step &st, unsigned m, int lane) {
+    int last = -1;
+#pragma unroll
+    for (int j = 0; j < kLaneVecs; ++j) {
+        if (st.v[j].x) last = (int)(st.v[j].y >> 2);
+        if (st.v[j].z) last = (int)(st.v[j].w >> 2);
+    }
+    const unsigned nb = group_ballot<G>(last >= 0, m, lane);
+    return nb ? group_bcast<G>(last, 31 - __clz(nb), m) : -1;
+}
+
+// Inside one step: the first entry whose running sum passes T, starting from
+// the running sum `base` before the step; the step's last non-zero entry when
+// rounding leaves the step short of T.
+template <int G>
+__device__ __forceinline__ int resolve_step(const Step &st, float base, float T, const float *ph, int gl, unsigned m,
+                                            int lane) {
+    float p[kLaneEntries];
+    step_probs(st, ph, p);
+    float cum = base + group_excl<G>(lane_sum(p), gl, m);
+    int hit = -1;
+#pragma unroll
+    for (int i = 0; i < kLaneEntries; ++i) {
+        cum += p[i];
+        const uint32_t cnt = (i & 1) ? st.v[i >> 1].z : st.v[i >> 1].x;
+        const uint32_t off = (i & 1) ? st.v[i >> 1].w : st.v[i >> 1].y;
+        if (hit < 0 && cnt && cum > T) hit = (int)(off >> 2);
+    }
+    const unsigned hb = group_ballot<G>(hit >= 0, m, lane);
+    if (hb) return group_bcast<G>(hit, __ffs(hb) - 1, m);
+    return step_last_nonzero<G>(st, m, lane);
+}
+
+// Pass 1 over the doc's theta row [rs, re): S as a compensated sum of the
+// group's step totals; lane 0 records the running sum after every step.  All
+// G lanes of a group see identical sums (butterfly reductions of the same
+// values), so they take the same branches and group-masked shuffles are safe.
+template <int G>
+__device__ __forceinline__ float row_sum(const ThetaEntry *__restrict__ theta, const float *ph, float *pref, int rs,
+                                         int re, int gl, unsigned m, int &nst_out) {
+    constexpr int kMax = SampleShape<G>::kMaxSteps, kStep = SampleShape<G>::kStep;
+    __syncwarp(m);  // the group's previous row is no longer being read from pref
+    float s = 0.f, c = 0.f;
+    int nst = 0;
+    for (int base = rs; base < re; base += kStep, ++nst) {
+        const Step st = load_step(theta, base + kLaneEntries * gl, re);
+        float p[kLaneEntries];
+        step_probs(st, ph, p);
+        neumaier(s, c, group_sum<G>(lane_sum(p), m));
+        if (gl == 0 && nst < kMax) pref[nst] = s + c;
+    }
+    __syncwarp(m);  // pref is complete before any lane searches it
+    nst_out = nst;
+    return s + c;
+}
+
+// The topic for target T = u * (S + Q): inverse CDF over the row (ascending
+// topic) when T < S, else over alpha * phihat (topics 0..K-1).
+template <int G>
+__device__ __forceinline__ int draw_topic(const ThetaEntry *__restrict__ theta, const float *ph, const float *qc,
+                                          const float *pref, int nst, float S, float T, int K, int rs, int re, int gl,
+                                          unsigned m, int lane) {
+    constexpr int kMax = SampleShape<G>::kMaxSteps, kStep = SampleShape<G>::kStep;
+    if (!(T < S)) return dense_bucket_search<G>(qc, K, T - S, gl, m, lane);
+    if (nst <= kMax) {
+        // the first step whose running sum passes T (the last one, S, does)
+        for (int r = 0; r < nst; r += G) {
+            const int j = r + gl;
+            const unsigned hb = group_ballot<G>(j < nst && pref[j] > T, m, lane);
+            if (hb) {
+                const int hs = r + __ffs(hb) - 1;
+                const float before = hs > 0 ? pref[hs - 1] : 0.f;
+                const Step st = load_step(theta, rs + hs * kStep + kLaneEntries * gl, re);
+                return resolve_step<G>(st, before, T, ph, gl, m, lane);
+            }
+        }
+    } else {
+        // long row: walk it again with the same arithmetic up to the step
+        // that passes T
+        float s2 = 0.f, c2 = 0.f;
+        for (int base = rs; base < re; base += kStep) {
+            const Step st = load_step(theta, base + kLaneEntries * gl, re);
+            float p[kLaneEntries];
+            step_probs(st, ph, p);
+            const float before = s2 + c2;
+            neumaier(s2, c2, group_sum<G>(lane_sum(p), m));
+            if (s2 + c2 > T) return resolve_step<G>(st, before, T, ph, gl, m, lane);
+        }
+    }
+    // Only reachable when T lies within the rounding of S itself: the token
+    // sits on the boundary between the buckets.  Take the row's last
+    // non-zero entry (it lies in the final 32-entry block).
+    int last = -1;
+    for (int i = max(rs, re - 32); i < re; ++i) {
+        const ThetaEntry e = __ldg(theta + i);
+        if (e.x) last = (int)(e.y >> 2);
+    }
+    return last;
+}
+
+// -------------------------------------------------------------- the kernel
+template <int G>
+__global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleParams p) {
+    extern __shared__ float smem[];
+    using Shape = SampleShape<G>;
+    const int K = p.k, KP = p.kmask + 1;
+    float *ph = smem;               // [KP] phihat of the current word (zero past K), at offset 0
+    float *inv = smem + KP;         // [K]  1 / (n_k + V beta)
+    float *qc = inv + K;            // [K]  dense-bucket prefix (the word histogram before that)
+    float *pref_all = qc + K;       // [kPrefixFloats] running sums per group
+    int *hist = reinterpret_cast<int *>(qc);
+    __shared__ int s_item;
+    __shared__ float s_warp[kSampleThreads / 32];
+    __shared__ double s_red[kSampleThreads / 32];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gl = lane & (G - 1);
+    const int group = tid / G;
+    constexpr int NG = Shape::kGroups;
+    float *pref = pref_all + group * Shape::kMaxSteps;
+    const unsigned m = group_mask<G>(lane);
+    const uint32_t iter = p.iteration_ptr ? *p.iteration_ptr : p.iteration;
+
+    for (int j = tid; j < K; j += blockDim.x) inv[j] = 1.0f / ((float)p.nk[j] + p.vbeta);
+    for (int j = K + tid; j < KP; j += blockDim.x) ph[j] = 0.f;
+
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(p.item_counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= p.num_items) break;
+        const culda_item item = p.items[it];
+        const int64_t ibeg = item.begin, iend = item.begin + item.count;
+        if (ibeg < 0 || item.count < 0 || iend > p.num_tokens || item.hot >= p.num_hot || item.seg_begin < 0 ||
+            item.seg_count < 0 || (int64_t)item.seg_begin + item.seg_count > p.num_segs) {
+            if (tid == 0) {
+                atomicOr(p.error, kErrRowRange);
+                p.item_ll[it] = 0.0;
+            }
+            __syncthreads();  // s_item is rewritten only after every thread has read it
+            continue;
+        }
+
+        // phi row of the word
+        const int *src;
+        if (item.hot < 0) {
+            for (int j = tid; j < K; j += blockDim.x) hist[j] = 0;
+            __syncthreads();
+            for (int64_t t = ibeg + tid; t < iend; t += blockDim.x) {
+                const uint32_t z = p.topics_in[t];
+                if (z < (uint32_t)K)
+                    atomicAdd(&hist[z], 1);
+                else
+                    atomicOr(p.error, kErrTopicRange);
+            }
+            __syncthreads();
+            src = hist;
+        } else {
+            src = p.hot_phi + (size_t)item.hot * K;
+        }
+        for (int j = tid; j < K; j += blockDim.x) ph[j] = ((float)src[j] + p.beta) * inv[j];
+        __syncthreads();
+        dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
+        __syncthreads();
+        const float Q = qc[K - 1];
+
+        double ll = 0.0;
+        const int sg_end = item.seg_begin + item.seg_count;
+        for (int sgb = item.seg_begin + group; sgb < sg_end; sgb += NG * G) {
+            // lane gl prefetches segment gl of this batch: its token range,
+            // doc and theta row
+            const int sgm = sgb + gl * NG;
+            int dm = -1, rsm = 0, rem = 0;
+            int64_t t0m = 0, t1m = 0;
+            if (sgm < sg_end) {
+                t0m = __ldg(p.seg_start + sgm);
+                t1m = sgm + 1 < sg_end ? (int64_t)__ldg(p.seg_start + sgm + 1) : iend;
+                if (t0m < ibeg || t1m > iend || t0m >= t1m) {
+                    atomicOr(p.error, kErrRowRange);
+                    t0m = t1m = 0;
+                } else {
+                    const int d = __ldg(p.doc_ids + t0m);
+                    if ((unsigned)d < (unsigned)p.num_docs) {
+                        const int2 r = __ldg(p.rows + d);
+                        if (r.x >= 0 && r.x <= r.y && (int64_t)r.y <= p.theta_cap && ((r.x | r.y) & 31) == 0) {
+                            dm = d;
+                            rsm = r.x;
+                            rem = r.y;
+                        } else {
+                            atomicOr(p.error, kErrRowRange);
+                        }
+                    } else {
+                        atomicOr(p.error, kErrDocRange);
+                    }
+                }
+            }
+#pragma unroll 1
+            for (int j = 0; j < G; ++j) {
+                if (sgb + j * NG >= sg_end) break;
+                const int d = group_bcast<G>(dm, j, m);
+                const int rs = group_bcast<G>(rsm, j, m), re = group_bcast<G>(rem, j, m);
+                const int64_t t0 = group_bcast<G>(t0m, j, m), t1 = group_bcast<G>(t1m, j, m);
+                if (d < 0) continue;
+                // every token of the segment shares the doc's row and so S,
+                // Q and the running sums; only its uniform differs
+                int nst;
+                const float S = row_sum<G>(p.theta, ph, pref, rs, re, gl, m, nst);
+                const float total = S + Q;
+                const double log_total = (double)logf(total);
+                for (int64_t tb = t0; tb < t1; tb += G) {
+                    // lane gl fetches the uniform of token tb + gl
+                    float um = 0.f;
+                    if (tb + gl < t1) {
+                        if (p.uniforms) {
+                            um = __ldg(p.uniforms + tb + gl);
+                        } else {
+                            const int64_t key = p.tok_index ? (int64_t)__ldg(p.tok_index + tb + gl) : tb + gl;
+                            um = uniform_from_bits(philox_token(p.seed, (uint64_t)key, iter, kPurposeSample));
+                        }
+                    }
+                    const int nb = (int)min((int64_t)G, t1 - tb);
+#pragma unroll 1
+                    for (int i = 0; i < nb; ++i) {
+                        const float T = group_bcast<G>(um, i, m) * total;
+                        int z = draw_topic<G>(p.theta, ph, qc, pref, nst, S, T, K, rs, re, gl, m, lane);
+                        if (gl == 0) {
+                            if (z < 0) {
+                                atomicOr(p.error, kErrRowRange);
+                                z = 0;
+                            }
+                            p.topics_out[tb + i] = (uint16_t)z;
+                            ll += log_total;
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ll += __shfl_down_sync(0xffffffffu, ll, o);
+        if (lane == 0) s_red[warp] = ll;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kSampleThreads / 32; ++w) s += s_red[w];
+            p.item_ll[it] = s;
+        }
+    }
+}
+
+size_t sample_smem_bytes(int k) {
+    // ph[pow2(K)] + inv[K] + qc[K] + the per-group running sums
+    return ((size_t)2 * k + (size_t)pow2_ceil(k) + (size_t)SampleShape<1>::kPrefixFloats) * sizeof(float);
+}
+
+template <int G>
+static const void *sample_fn() {
+    return reinterpret_cast<const void *>(&sample_kernel<G>);
+}
+
+static const void *sample_kernel_for(int g) {
+    switch (g) {
+        case 1: return sample_fn<1>();
+        case 2: return sample_fn<2>();
+        case 4: return sample_fn<4>();
+        case 8: return sample_fn<8>();
+        case 16: return sample_fn<16>();
+        case 32: return sample_fn<32>();
+        default: return nullptr;
+    }
+}
+
+int sample_blocks_per_sm(int k, int group_lanes) {
+    const void *fn = sample_kernel_for(group_lanes);
+    if (!fn) return 0;
+    const size_t smem = sample_smem_bytes(k);
+    if (allow_smem(fn, smem, nullptr) != cudaSuccess) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kSampleThreads, smem) != cudaSuccess) return 0;
+    return n;
+}
+
+cudaError_t launch_sample(const SampleParams &p, int group_lanes, int grid, cudaStream_t s) {
+    const size_t smem = sample_smem_bytes(p.k);
+    void *args[] = {const_cast<SampleParams *>(&p)};
+    const void *fn = sample_kernel_for(group_lanes);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaError_t e = allow_smem(fn, smem, s);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernel(fn, dim3(grid), dim3(kSampleThreads), args, smem, s);
+}
+
+// ----------------------------------------------------------- hot-word rows
+// Full phi rows of words split over several work items: each CTA histograms
+// one slice in shared memory and adds the non-zero bins to the word's row.
+__global__ void __launch_bounds__(256) hot_rows_kernel(int K, const culda_item *__restrict__ hot_items,
+                                                       const uint16_t *__restrict__ topics, int32_t *hot_phi,
+                                                       int32_t *error) {
+    extern __shared__ int hist_s[];
+    const culda_item it = hot_items[blockIdx.x];
+    for (int j = threadIdx.x; j < K; j += blockDim.x) hist_s[j] = 0;
+    __syncthreads();
+    for (int64_t t = it.begin + threadIdx.x; t < it.begin + it.count; t += blockDim.x) {
+        const uint32_t z = topics[t];
+        if (z < (uint32_t)K)
+            atomicAdd(&hist_s[z], 1);
+        else
+            atomicOr(error, kErrTopicRange);
+    }
+    __syncthreads();
+    int32_t *row = hot_phi + (size_t)it.hot * K;
+    for (int j = threadIdx.x; j < K; j += blockDim.x)
+        if (hist_s[j]) atomicAdd(&row[j], hist_s[j]);
+}
+
+cudaError_t launch_hot_rows(int k, const culda_item *hot_items, int num_hot_items, const uint16_t *topics,
+                            int32_t *hot_phi, int32_t *error, cudaStream_t s) {
+    if (num_hot_items <= 0) return cudaSuccess;
+    const size_t smem = (size_t)k * sizeof(int);
+    cudaError_t e = allow_smem(reinterpret_cast<const void *>(&hot_rows_kernel), smem, s);
+    if (e != cudaSuccess) return e;
+    hot_rows_kernel<<<num_hot_items, 256, smem, s>>>(k, hot_items, topics, hot_phi, error);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- LL finalize
+__global__ void __launch_bounds__(256) finalize_ll_kernel(const double *__restrict__ item_ll, int num_items,
+                                                          DevStats *st, uint32_t *iteration_dev) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < num_items; i += 256) s += item_ll[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        st->ll_sum = red[0];
+        if (iteration_dev) {
+            st->iteration = *iteration_dev;
+            *iteration_dev += 1u;
+        }
+    }
+}
+
+cudaError_t launch_finalize_ll(const double *item_ll, int num_items, DevStats *st, uint32_t *iteration_dev,
+                               cudaStream_t s) {
+    finalize_ll_kernel<<<1, 256, 0, s>>>(item_ll, num_items, st, iteration_dev);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------- theta entry validation
+// Every entry of every row must carry a topic below K (as a byte offset) and
+// rows must be 32-aligned inside the array: checked before the kernel-level
+// entry point samples a caller's theta.
+__global__ void check_theta_kernel(int num_docs, int K, const int2 *__restrict__ rows,
+                                   const ThetaEntry *__restrict__ theta, int64_t cap, int32_t *error) {
+    const int lane = threadIdx.x & 31;
+    for (int d = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; d < num_docs; d += (gridDim.x * blockDim.x) >> 5) {
+        const int2 r = rows[d];
+        if (r.x < 0 || r.y < r.x || (int64_t)r.y > cap || ((r.x | r.y) & 31)) {
+            if (lane == 0) atomicOr(error, kErrRowRange);
+            continue;
+        }
+        for (int i = r.x + lane; i < r.y; i += 32) {
+            const ThetaEntry e = theta[i];
+            if ((e.y & 3u) || (e.y >> 2) >= (uint32_t)K) atomicOr(error, kErrTopicRange);
+        }
+    }
+}
+
+cudaError_t launch_check_theta(int num_docs, int k, const int2 *rows, const ThetaEntry *theta, int64_t cap,
+                               int32_t *error, cudaStream_t s) {
+    check_theta_kernel<<<grid_for((int64_t)num_docs * 32), 256, 0, s>>>(num_docs, k, rows, theta, cap, error);
+    return cudaGetLastError();
+}
+
+}  // namespace culda

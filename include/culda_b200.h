@@ -27,9 +27,13 @@
  *   doc_ptr   int64[D+1]  token count prefix per doc (reference: docRevIndices)
  *   doc_tok   int32[N]    word-major token index of every token, grouped by doc
  *                         and ascending within a doc (reference: docRevIdx)
- *   theta     uint32[cap] packed CSR entry (count << 16) | topic, ascending
- *                         topic inside a row, zero padded (reference: thetaA and
- *                         thetaJA, two int16 arrays, lda_theta_kernel.cu:55-58)
+ *   theta     uint32[2*cap] CSR entries of two words: {float bits of the
+ *                         count, 4 * topic}, ascending topic inside a row, zero
+ *                         padded (reference: thetaA and thetaJA, two int16
+ *                         arrays, lda_theta_kernel.cu:55-58).  The count is kept
+ *                         as a float and the topic as a byte offset so the
+ *                         sampler needs one shared-memory load and one multiply
+ *                         per entry.
  *   theta_rows int32[2*D] {row start, row end} per doc; start is the reference's
  *                         thetaMaxIA[d], end its thetaCurIA[d] = start + roundup32(nnz)
  *   nk        int32[K]    tokens per topic (reference: phiTopic)
@@ -148,7 +152,8 @@ typedef struct culda_params {
 
 enum {
     CULDA_FLAG_NO_GRAPH = 1,      /* launch the iteration kernel by kernel instead of one CUDA graph */
-    CULDA_FLAG_VERBOSE = 2        /* print set-up details to stderr */
+    CULDA_FLAG_VERBOSE = 2,       /* print set-up details to stderr */
+    CULDA_FLAG_NO_REORDER = 4     /* keep tokens in input order inside each word (default: by doc length) */
 };
 
 typedef struct culda_iter_stats {
@@ -233,7 +238,9 @@ typedef struct culda_item {
     int32_t count;
     int32_t word;
     int32_t hot;
-    int32_t first;  /* 1 on the first item of its word */
+    int32_t first;      /* 1 on the first item of its word */
+    int32_t seg_begin;  /* the item's segments are seg_start[seg_begin .. seg_begin+seg_count) */
+    int32_t seg_count;
 } culda_item;
 
 /* Build the work list for `word_ptr` (host).  Items are ordered largest first.
@@ -241,6 +248,15 @@ typedef struct culda_item {
  * items == NULL only counts.  *num_hot receives the number of hot words. */
 int64_t culda_build_items(int32_t num_words, const int64_t *word_ptr, int32_t item_tokens,
                           culda_item *items, int64_t max_items, int32_t *num_hot);
+
+/* Segments of a work list (host): maximal runs of consecutive tokens of one
+ * doc inside an item, at most max_len tokens each.  Tokens of one word in one
+ * doc share their sampling distribution on a frozen snapshot, so the sampler
+ * walks the doc's theta row once per segment.  Fills seg_begin/seg_count of
+ * every item and seg_start (the first token of each segment); returns the
+ * number of segments or a negative status; with seg_start == NULL only counts. */
+int64_t culda_build_segments(int64_t num_tokens, const int32_t *doc_ids, culda_item *items, int32_t num_items,
+                             int32_t max_len, int32_t *seg_start, int64_t max_segs);
 
 /* Replaces LDAUpdatePhiAPI (src_culda/kernel/lda_phi_kernel.cu:136-159) and the
  * n_k memset before it (src_culda/model/model_phi_gpu.cpp:79).  Per-word shared
@@ -285,7 +301,9 @@ typedef struct culda_sample_args {
     const uint32_t *theta;       /* packed CSR of the snapshot */
     const int32_t *theta_rows;   /* [2*D] */
     const int32_t *nk;           /* [K] of the snapshot */
-    const culda_item *items;     /* device copy of the work list */
+    const culda_item *items;     /* device copy of the work list (with segments) */
+    const int32_t *seg_start;    /* device copy of the segment starts (culda_build_segments) */
+    int32_t num_segs;
     int32_t num_items;
     int32_t num_hot;             /* words split over several items */
     const culda_item *hot_items; /* device copy of the items with hot >= 0 (any order) */

@@ -372,6 +372,69 @@ void oracle_sample_fp64(int32_t num_docs, int32_t num_words, int32_t k, float al
     }
 }
 
+/* ------------------------------------------- reference-compatible loglik */
+/*
+ * The value the reference prints (lda_train_kernel.cu:56-262 then
+ * LDATrainPerplexity :273-356), with its own arithmetic:
+ *   - phiHeadCache = FP16 phiHead widened to float (lda_train_kernel.cu:71),
+ *     FP16 rounding of the float quotient (lda_phi_kernel.cu:26-29);
+ *   - Q: per group of 32 topics a shfl_down tree of alpha*phi (16,8,4,2,1),
+ *     then a lock-step Kogge-Stone scan of the 32 group sums (:68-99);
+ *   - S: per 32-entry chunk of the doc's row a shfl_down tree of A*phi,
+ *     accumulated chunk by chunk in float (:116-137);
+ *   - term = logf((S+Q) / (float)(L_d + K*alpha)) summed in float by each warp
+ *     over tokens start+w, start+w+32, ... of its slot (:104-106,256-262);
+ *   - each warp sum truncated to int, only the first numWords*32 warp slots
+ *     summed (:282-298, :338), divided by N (:355).
+ * slot_word / slot_range are the slots of DocChunk::loadChunk (doc_chunk.cpp:148-205).
+ */
+static inline float warp_tree32(const float *v) {
+    float a[32];
+    for (int l = 0; l < 32; ++l) a[l] = v[l];
+    for (int o = 16; o >= 1; o >>= 1)
+        for (int l = 0; l < o; ++l) a[l] = a[l] + a[l + o];
+    return a[0];
+}
+
+double oracle_loglik_reference(int32_t num_words, int32_t k, float alpha, int64_t num_tokens, int32_t num_slots,
+                               const int32_t *slot_word, const int64_t *slot_range, const int32_t *doc_ids,
+                               const int64_t *doc_ptr, const uint16_t *phi_head, const int16_t *theta_a,
+                               const int16_t *theta_ja, const int32_t *max_ia, const int32_t *cur_ia) {
+    std::vector<float> cache((size_t)k), qtree(32);
+    int64_t total = 0;
+    for (int32_t s = 0; s < num_slots; ++s) {
+        const int32_t w = slot_word[s];
+        for (int32_t j = 0; j < k; ++j) cache[j] = oracle_half_to_float(phi_head[(size_t)w * k + j]);
+        float grp[32];
+        for (int g = 0; g < 32; ++g) {
+            for (int l = 0; l < 32; ++l) grp[l] = 32 * g + l < k ? alpha * cache[32 * g + l] : 0.f;
+            qtree[g] = warp_tree32(grp);
+        }
+        for (int o = 1; o < 32; o <<= 1) {
+            float nv[32];
+            for (int l = 0; l < 32; ++l) nv[l] = l >= o ? qtree[l - o] + qtree[l] : qtree[l];
+            for (int l = 0; l < 32; ++l) qtree[l] = nv[l];
+        }
+        const float Q = qtree[31];
+        for (int warp = 0; warp < 32; ++warp) {
+            float sum = 0.0f;
+            for (int64_t t = slot_range[2 * s] + warp; t < slot_range[2 * s + 1]; t += 32) {
+                const int32_t d = doc_ids[t];
+                float S = 0.f;
+                for (int32_t base = max_ia[d]; base < cur_ia[d]; base += 32) {
+                    float p[32];
+                    for (int l = 0; l < 32; ++l) p[l] = (float)(int)theta_a[base + l] * cache[(uint16_t)theta_ja[base + l]];
+                    S += warp_tree32(p);
+                }
+                const float den = (float)(doc_ptr[d + 1] - doc_ptr[d]) + (float)k * alpha;
+                sum += logf((S + Q) / den);
+            }
+            if (s < num_words) total += (int64_t)(int)(double)sum;
+        }
+    }
+    return (double)total / (double)num_tokens;
+}
+
 /* ------------------------------------------------------ joint likelihood */
 /*
  * log p(w, z) = K lgamma(V b) - sum_k lgamma(n_k + V b) + sum_{w,k: n>0} [lgamma(n_wk + b) - lgamma(b)]

@@ -108,3 +108,39 @@ def test_build_items_splits_hot_words_and_covers_every_token():
         assert (hot >= 0) == (lens[w] > 2500)
     assert (covered == 1).all()
     assert sum(it[4] for it in items) == int((lens > 0).sum())  # one first item per non-empty word
+
+
+def test_build_segments_runs_of_one_doc_inside_items():
+    lens = np.array([70, 5, 1, 40])
+    wp = np.concatenate([[0], np.cumsum(lens)])
+    # word 0: doc 3 x 70 (one long run), word 1: docs 1,1,2,2,2, word 2: doc 0, word 3: docs 4 x 40
+    doc_ids = np.array([3] * 70 + [1, 1, 2, 2, 2] + [0] + [4] * 40, dtype=np.int32)
+    items = build_items_struct(wp, 50)
+    lib = cb.lib()
+    n = lib.culda_build_segments(len(doc_ids), doc_ids.ctypes.data_as(C.POINTER(C.c_int32)), items, len(items), 32,
+                                 None, 0)
+    seg = np.zeros(n, dtype=np.int32)
+    assert lib.culda_build_segments(len(doc_ids), doc_ids.ctypes.data_as(C.POINTER(C.c_int32)), items, len(items),
+                                    32, seg.ctypes.data_as(C.POINTER(C.c_int32)), n) == n
+    covered = np.zeros(len(doc_ids), dtype=int)
+    for it in items:
+        starts = list(seg[it.seg_begin:it.seg_begin + it.seg_count]) + [it.begin + it.count]
+        assert starts[0] == it.begin
+        for a, b in zip(starts[:-1], starts[1:]):
+            assert 0 < b - a <= 32 and (doc_ids[a:b] == doc_ids[a]).all()
+            covered[a:b] += 1
+    assert (covered == 1).all()
+    # word 0 (70 tokens of one doc) is split into two items of 35, each cut into 32 + 3;
+    # word 1 -> 2 (docs 1 and 2); word 2 -> 1; word 3 (40 of one doc) -> 32 + 8
+    assert n == 4 + 2 + 1 + 2
+
+
+def build_items_struct(word_ptr, item_tokens):
+    wp = np.ascontiguousarray(word_ptr, dtype=np.int64)
+    lib = cb.lib()
+    nhot = C.c_int32()
+    n = lib.culda_build_items(len(wp) - 1, wp.ctypes.data_as(C.POINTER(C.c_int64)), item_tokens, None, 0,
+                              C.byref(nhot))
+    items = (_ffi.Item * n)()
+    lib.culda_build_items(len(wp) - 1, wp.ctypes.data_as(C.POINTER(C.c_int64)), item_tokens, items, n, C.byref(nhot))
+    return items

@@ -25,6 +25,7 @@ CULDA_ERR_DEVICE_STATE = -7
 CULDA_ERR_NO_DEVICE = -8
 
 CULDA_LEN_POISSON, CULDA_LEN_LOGNORMAL, CULDA_LEN_PARETO = 0, 1, 2
+CULDA_NOALLOC_SCRATCH_BYTES = 8 << 20  # include/culda_b200.h
 CULDA_FLAG_NO_GRAPH, CULDA_FLAG_VERBOSE, CULDA_FLAG_NO_REORDER = 1, 2, 4
 
 
@@ -104,6 +105,7 @@ SIGNATURES = {
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     "culda_sample_workspace": (C.c_size_t, [i32, i32, i32]),
     "culda_sample": (C.c_int, [P(SampleArgs), C.c_void_p, C.c_size_t, C.c_void_p]),
+    "culda_sample_noalloc": (C.c_int, [P(SampleArgs), C.c_void_p]),
     "culda_loglik": (C.c_int, [C.c_void_p, f64, i64, P(f64), C.c_void_p]),
 }
 

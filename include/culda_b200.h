@@ -327,6 +327,26 @@ size_t culda_sample_workspace(int32_t k, int32_t num_items, int32_t num_hot);
  * draw by inverse CDF over the row (ascending topic) then over 0..K-1. */
 int culda_sample(const culda_sample_args *a, void *d_workspace, size_t workspace_bytes, void *stream);
 
+/* Size of the fixed device scratch array behind culda_sample_noalloc (8 MiB,
+ * held on every GPU that loads the library until the process exits). */
+#define CULDA_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+/* culda_sample without a caller workspace; no counterpart in the reference.
+ * For callers that cannot allocate device memory for the sampler: an
+ * application whose own pool allocator owns all device memory and does not
+ * let libraries call cudaMalloc, or a latency-sensitive loop that cannot pay
+ * the device-wide synchronisation of an allocation.  Same arguments, checks
+ * and results as culda_sample; the scratch is a fixed device array of
+ * CULDA_NOALLOC_SCRATCH_BYTES instead of a workspace, and the call allocates
+ * nothing.  A work list needing more scratch than that (culda_sample_workspace)
+ * is rejected with CULDA_ERR_UNSUPPORTED.  The first call on each device looks
+ * up the array's device address (and loads the library's device code there if
+ * that has not happened yet): make that first call before any stream capture.
+ * Every call on a device shares the one array, so calls that may overlap on
+ * the GPU (other streams, other host threads) race and must be serialised by
+ * the caller. */
+int culda_sample_noalloc(const culda_sample_args *a, void *stream);
+
 /* Replaces LDATrainPerplexity (src_culda/kernel/lda_train_kernel.cu:323-356):
  * turns the device sum written by culda_sample into the per-token value the
  * reference prints: (sum - sum_d L_d*log(L_d + K*alpha)) / N, read back to

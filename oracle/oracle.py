@@ -215,3 +215,16 @@ class Snapshot:
                          self.theta_a if theta_a is None else theta_a, self.theta_ja if theta_ja is None else theta_ja,
                          self.max_ia, self.cur_ia if cur_ia is None else cur_ia)
         return vp, vt
+
+
+def loglik_reference(snapshot: "Snapshot", num_tokens: int, slot_word, slot_range, phi_head_f16_table) -> float:
+    """The log-likelihood the reference prints (oracle_loglik_reference)."""
+    s = snapshot
+    f = lib().oracle_loglik_reference
+    f.restype = C.c_double
+    sw = _c(slot_word, np.int32)
+    sr = _c(slot_range, np.int64)
+    ph = _c(phi_head_f16_table, np.uint16)
+    return f(C.c_int32(s.num_words), C.c_int32(s.k), C.c_float(s.alpha), C.c_int64(num_tokens), C.c_int32(len(sw)),
+             _p(sw), _p(sr), _p(s.doc_ids), _p(s.doc_ptr), _p(ph), _p(s.theta_a), _p(s.theta_ja), _p(s.max_ia),
+             _p(s.cur_ia))

@@ -185,8 +185,8 @@ def ncu_traffic(workload: str):
     if not p.exists():
         return None
     try:
-        d = json.loads(p.read_text())
-        return d.get(workload)
+        d = json.loads(p.read_text()).get(workload)
+        return int(d["dram_bytes_per_launch"]) if d else None
     except Exception:
         return None
 
@@ -235,7 +235,9 @@ def run_ours(args, world, rank, local, pg):
     prev = ([warm[-1]] if warm else []) + stats[:-1]
     if len(prev) < len(stats):  # no warm-up: the first sampler walked the initial rows
         prev = [stats[0]] + prev
-    sample_bytes = [16 * N + 4 * p["token_nnz"] + 4 * info["num_hot_items"] * 0 for p in prev]
+    sample_bytes = [16 * N + 4 * p["token_nnz"] for p in prev]
+    # each array once: doc ids, topics in and out, uniforms, theta entries, row pointers
+    compulsory = [12 * N + 8 * p["theta_nnz"] + 8 * corpus.num_docs for p in prev]
     sample_sec = [s["sample_seconds"] for s in stats]
     achieved = sum(sample_bytes) / sum(sample_sec) / 1e9
     peak, peak_kind = measured_peaks()
@@ -245,7 +247,12 @@ def run_ours(args, world, rank, local, pg):
                 "traffic": traffic, "bytes_per_launch": int(statistics.mean(sample_bytes)),
                 "launch_ms": round(1e3 * statistics.mean(sample_sec), 4),
                 "rebuild_ms": round(1e3 * statistics.mean(s["rebuild_seconds"] for s in stats), 4),
-                "formula": "sum_t (4 doc id + 2 topic in + 2 topic out + 8 row) + 4 * sum_t nnz(row of d(t))"}
+                "formula": "sum_t (4 doc id + 2 topic in + 2 topic out + 8 row) + 4 * sum_t nnz(row of d(t))",
+                "compulsory_bytes_per_launch": int(statistics.mean(compulsory)),
+                "compulsory_frac": round(sum(compulsory) / sum(sample_sec) / 1e9 / peak, 4),
+                "compulsory_formula": "12 N (doc id, topic in, topic out, uniform) + 8 nnz(theta) + 8 D (rows)",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                  "profiles/sample_kernel_traffic.json" if traffic else None}
     m.close()
 
     # ---- end to end through the public API from pinned host buffers

@@ -503,7 +503,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         CKB(dalloc(&keys_out, (size_t)N));
         CKB(dalloc(&vals, (size_t)N));
         CKB(dalloc(&ctx->d_tok_index, (size_t)N));
-        CKB(launch_order_keys(V, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, keys, s));
+        CKB(launch_order_keys(V, N, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, keys, s));
         CKB(launch_iota(N, vals, s));
         int end_bit = 17;
         while ((1ll << (end_bit - 16)) < (int64_t)V) ++end_bit;

@@ -209,22 +209,32 @@ cudaError_t launch_check_topics(int64_t n, int k, const uint16_t *z, int32_t *er
     return cudaGetLastError();
 }
 
-// Warp per word: the sort key of each of its tokens.
-__global__ void order_keys_kernel(int num_words, const int64_t *__restrict__ word_ptr,
+// Thread per token: the word is found by binary search of word_ptr (V+1
+// ascending offsets, L2-resident), so a Zipf-head word of millions of tokens
+// is spread over the whole grid instead of one warp.
+__global__ void order_keys_kernel(int num_words, int64_t num_tokens, const int64_t *__restrict__ word_ptr,
                                   const int32_t *__restrict__ doc_ids, const int64_t *__restrict__ doc_ptr,
                                   uint64_t *keys) {
-    const int lane = threadIdx.x & 31;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < num_words; w += (gridDim.x * blockDim.x) >> 5)
-        for (int64_t t = word_ptr[w] + lane; t < word_ptr[w + 1]; t += 32) {
-            const int d = doc_ids[t];
-            const int64_t len = min(doc_ptr[d + 1] - doc_ptr[d], (int64_t)65535);
-            keys[t] = ((uint64_t)w << 16) | (uint64_t)(65535 - len);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < num_tokens;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = num_words - 1;  // the last word w with word_ptr[w] <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(word_ptr + mid) <= t)
+                lo = mid;
+            else
+                hi = mid - 1;
         }
+        const int d = doc_ids[t];
+        const int64_t len = min(doc_ptr[d + 1] - doc_ptr[d], (int64_t)65535);
+        keys[t] = ((uint64_t)lo << 16) | (uint64_t)(65535 - len);
+    }
 }
 
-cudaError_t launch_order_keys(int num_words, const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr,
-                              uint64_t *keys, cudaStream_t s) {
-    order_keys_kernel<<<148 * 16, 256, 0, s>>>(num_words, word_ptr, doc_ids, doc_ptr, keys);
+cudaError_t launch_order_keys(int num_words, int64_t num_tokens, const int64_t *word_ptr, const int32_t *doc_ids,
+                              const int64_t *doc_ptr, uint64_t *keys, cudaStream_t s) {
+    if (num_tokens <= 0) return cudaSuccess;
+    order_keys_kernel<<<grid_for(num_tokens), 256, 0, s>>>(num_words, num_tokens, word_ptr, doc_ids, doc_ptr, keys);
     return cudaGetLastError();
 }
 

@@ -104,8 +104,8 @@ cudaError_t launch_loglik_joint(int k, int num_words, int num_docs, float alpha,
 
 // Internal token order: within each word, tokens sorted by their doc's length
 // (longest first, doc id breaking ties).  keys[t] = (word << 16) | (65535 - L).
-cudaError_t launch_order_keys(int num_words, const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr,
-                              uint64_t *keys, cudaStream_t s);
+cudaError_t launch_order_keys(int num_words, int64_t num_tokens, const int64_t *word_ptr, const int32_t *doc_ids,
+                              const int64_t *doc_ptr, uint64_t *keys, cudaStream_t s);
 template <class T>
 cudaError_t launch_gather(int64_t n, const int32_t *index, const T *src, T *dst, cudaStream_t s);
 template <class T>

@@ -209,7 +209,8 @@ def run_ours(args, world, rank, local, pg):
 
     # ---- device-resident measurement
     m = cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed + rank, device=local, group_lanes=args.group_lanes,
-               item_tokens=args.item_tokens)
+               item_tokens=args.item_tokens, sample_blocks=args.sample_blocks,
+               flags=cb.CULDA_FLAG_AUTOTUNE if args.autotune else 0)
     info = m.info()
     log(f"[rank {rank}] info {info}")
     clocks = ClockSampler(local)
@@ -271,7 +272,8 @@ def run_ours(args, world, rank, local, pg):
         cuda_sync()
         t0 = time.perf_counter()
         m2 = cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed + rank, device=local,
-                    group_lanes=args.group_lanes, item_tokens=args.item_tokens)
+                    group_lanes=args.group_lanes, item_tokens=args.item_tokens, sample_blocks=args.sample_blocks,
+                    flags=cb.CULDA_FLAG_AUTOTUNE if args.autotune else 0)
         lls = [s["loglik"] for s in m2.iterate(args.steps)]
         st = cb.lib().culda_get_topics(m2._ctx, C.cast(z_host.data_ptr(), C.POINTER(C.c_uint16)))
         cuda_sync()
@@ -313,7 +315,9 @@ def run_ours(args, world, rank, local, pg):
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded generator, shapes of the workload)",
         "config": {"workload": wl.name, "num_tokens": N, "num_docs": corpus.num_docs, "num_words": corpus.num_words,
                    "k": wl.k, "alpha": wl.alpha, "beta": wl.beta, "seed": args.seed,
-                   "group_lanes": info["group_lanes"], "items": info["num_items"], "hot_words": info["num_hot"],
+                   "group_lanes": info["group_lanes"], "sample_blocks": info["sample_blocks"],
+                   "autotuned": bool(info["tuned"]),
+                   "items": info["num_items"], "hot_words": info["num_hot"],
                    "l2": f"inputs larger than L2 (resident set {info['device_bytes'] / 1e9:.2f} GB > 126 MB)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
@@ -391,6 +395,8 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--group-lanes", type=int, default=0)
     ap.add_argument("--item-tokens", type=int, default=0)
+    ap.add_argument("--sample-blocks", type=int, default=0, help="sampler register budget (CTAs per SM): 0, 8, 10")
+    ap.add_argument("--autotune", action="store_true", help="time the sampler variants at create and keep the fastest")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iterations", type=int, default=2)

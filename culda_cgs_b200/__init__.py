@@ -5,7 +5,7 @@ include/culda_b200.h (libculda_b200.so); this package is a thin ctypes host
 over it that mirrors the reference's host interface (Document, Argument,
 LDATrain).
 """
-from ._ffi import CuldaError, lib, library_path
+from ._ffi import CULDA_FLAG_AUTOTUNE, CULDA_FLAG_NO_GRAPH, CULDA_FLAG_NO_REORDER, CULDA_FLAG_VERBOSE, CuldaError, lib, library_path
 from .corpus import BorrowedCorpus, Corpus, Document, GenConfig
 from .lda import LDA, Argument, LDATrain
 

@@ -26,7 +26,7 @@ CULDA_ERR_NO_DEVICE = -8
 
 CULDA_LEN_POISSON, CULDA_LEN_LOGNORMAL, CULDA_LEN_PARETO = 0, 1, 2
 CULDA_NOALLOC_SCRATCH_BYTES = 8 << 20  # include/culda_b200.h
-CULDA_FLAG_NO_GRAPH, CULDA_FLAG_VERBOSE, CULDA_FLAG_NO_REORDER = 1, 2, 4
+CULDA_FLAG_NO_GRAPH, CULDA_FLAG_VERBOSE, CULDA_FLAG_NO_REORDER, CULDA_FLAG_AUTOTUNE = 1, 2, 4, 8
 
 
 class Corpus(C.Structure):
@@ -42,7 +42,7 @@ class GenParams(C.Structure):
 
 class Params(C.Structure):
     _fields_ = [("k", i32), ("alpha", f32), ("beta", f32), ("seed", u64), ("device", i32), ("group_lanes", i32),
-                ("item_tokens", i32), ("flags", i32)]
+                ("item_tokens", i32), ("flags", i32), ("sample_blocks", i32)]
 
 
 class IterStats(C.Structure):
@@ -53,8 +53,10 @@ class IterStats(C.Structure):
 
 class Info(C.Structure):
     _fields_ = [("num_items", i32), ("num_hot", i32), ("num_hot_items", i32), ("item_tokens", i32),
-                ("group_lanes", i32), ("sample_grid", i32), ("theta_grid", i32), ("kernels_per_iteration", i32),
-                ("theta_capacity", i64), ("device_bytes", i64), ("doc_term", f64)]
+                ("group_lanes", i32), ("sample_grid", i32), ("sample_blocks", i32), ("theta_grid", i32),
+                ("kernels_per_iteration", i32),
+                ("theta_capacity", i64), ("device_bytes", i64), ("doc_term", f64), ("tuned", i32),
+                ("tune_ms", f32)]
 
 
 class Item(C.Structure):

@@ -19,7 +19,11 @@
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <fstream>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -35,6 +39,10 @@ struct culda_ctx {
     int32_t D = 0, V = 0, K = 0;
     int64_t N = 0;
     int group_lanes = 8;
+    int sample_blocks = kSampleBlocksDefault;
+    int tuned = 0;
+    bool tune_pending = false;  // time the variants before iteration kTuneIteration
+    float tune_ms = 0.f;
     int item_tokens = 0;
 
     int64_t *d_word_ptr = nullptr, *d_doc_ptr = nullptr;
@@ -75,6 +83,64 @@ struct culda_ctx {
 };
 
 namespace {
+
+// ------------------------------------------------------------ autotuner
+// Sampler variants are timed on the context's initial state; the fastest is
+// kept.  Results are remembered per (device name, N, D, V, K): in the process,
+// and in the file named by CULDA_TUNE_CACHE (lines "key group_lanes
+// sample_blocks ms") when that variable is set.
+struct TuneResult {
+    int group_lanes = 0, sample_blocks = 0;
+    float ms = 0.f;
+};
+
+std::mutex g_tune_mu;
+std::map<std::string, TuneResult> g_tune_cache;
+
+std::string tune_key(const culda_ctx *ctx) {
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) prop.name[0] = 0;
+    std::ostringstream k;
+    std::string name(prop.name);
+    std::replace(name.begin(), name.end(), ' ', '_');
+    k << name << ":N" << ctx->N << ":D" << ctx->D << ":V" << ctx->V << ":K" << ctx->K;
+    return k.str();
+}
+
+bool tune_lookup(const std::string &key, TuneResult &r) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+        r = it->second;
+        return true;
+    }
+    const char *path = std::getenv("CULDA_TUNE_CACHE");
+    if (!path || !*path) return false;
+    std::ifstream f(path);
+    std::string line;
+    bool found = false;
+    while (std::getline(f, line)) {
+        std::istringstream ls(line);
+        std::string k;
+        TuneResult t;
+        if (ls >> k >> t.group_lanes >> t.sample_blocks >> t.ms && k == key && sample_variant_exists(t.group_lanes, t.sample_blocks)) {
+            r = t;
+            found = true;  // the last line for a key wins
+        }
+    }
+    if (found) g_tune_cache[key] = r;
+    return found;
+}
+
+void tune_store(const std::string &key, const TuneResult &r) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = r;
+    const char *path = std::getenv("CULDA_TUNE_CACHE");
+    if (!path || !*path) return;
+    std::ofstream f(path, std::ios::app);
+    f << key << ' ' << r.group_lanes << ' ' << r.sample_blocks << ' ' << r.ms << '\n';
+}
+
 
 int fail(culda_ctx *c, int code, const char *fmt, ...) {
     char buf[512];
@@ -158,7 +224,8 @@ int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
     }
     CK(launch_uniforms(ctx->N, ctx->params.seed, ctx->d_iter, 0u, ctx->d_tok_index, ctx->d_u, s));
     CK(record_event(ctx->ev_s0, s));
-    CK(launch_sample(sample_params(ctx, cur, 0u, ctx->d_iter), ctx->group_lanes, ctx->sample_grid, s));
+    CK(launch_sample(sample_params(ctx, cur, 0u, ctx->d_iter), ctx->group_lanes, ctx->sample_blocks,
+                     ctx->sample_grid, s));
     CK(record_event(ctx->ev_s1, s));
     CK(launch_finalize_ll(ctx->d_item_ll, ctx->num_items, ctx->d_stats, ctx->d_iter, s));
     CK(cudaMemsetAsync(ctx->d_nk, 0, sizeof(int32_t) * (size_t)ctx->K, s));
@@ -189,6 +256,75 @@ int rebuild_counts(culda_ctx *ctx) {
     return CULDA_OK;
 }
 
+constexpr uint32_t kTuneIteration = 3;
+
+// Times each sampler variant on the current state: hot rows and
+// uniforms once, then per variant one warm-up and two timed launches that
+// write the other topic buffer.  The context's state does not change.
+int autotune_sampler(culda_ctx *ctx) {
+    static const int kCands[][2] = {{4, kSampleBlocksHigh}, {8, kSampleBlocksHigh}, {16, kSampleBlocksHigh},
+                                    {2, kSampleBlocksDefault}, {4, kSampleBlocksDefault}, {8, kSampleBlocksDefault}};
+    const std::string key = tune_key(ctx);
+    TuneResult best;
+    if (tune_lookup(key, best)) {
+        const int bps = sample_blocks_per_sm(ctx->K, best.group_lanes, best.sample_blocks);
+        if (bps > 0) {
+            ctx->group_lanes = best.group_lanes;
+            ctx->sample_blocks = best.sample_blocks;
+            ctx->sample_grid = std::max(1, std::min(ctx->num_items, num_sms(ctx->device) * bps));
+            ctx->tuned = 2;
+            ctx->tune_ms = best.ms;
+            return CULDA_OK;
+        }
+    }
+    cudaStream_t s = ctx->stream;
+    const int cur = ctx->cur;
+    if (ctx->num_hot > 0) {
+        CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
+        CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
+                           s));
+    }
+    CK(launch_uniforms(ctx->N, ctx->params.seed, nullptr, 1u, ctx->d_tok_index, ctx->d_u, s));
+    const SampleParams sp = sample_params(ctx, cur, 1u, nullptr);
+    best.ms = 0.f;
+    for (const auto &c : kCands) {
+        const int bps = sample_blocks_per_sm(ctx->K, c[0], c[1]);
+        if (bps <= 0) continue;
+        const int grid = std::max(1, std::min(ctx->num_items, num_sms(ctx->device) * bps));
+        float t = 0.f;
+        for (int rep = 0; rep < 3; ++rep) {
+            CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
+            CK(cudaEventRecord(ctx->ev0, s));
+            CK(launch_sample(sp, c[0], c[1], grid, s));
+            CK(cudaEventRecord(ctx->ev1, s));
+            CK(cudaEventSynchronize(ctx->ev1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            if (rep == 1 || (rep == 2 && ms < t)) t = ms;
+        }
+        if (best.ms == 0.f || t < best.ms) {
+            best.group_lanes = c[0];
+            best.sample_blocks = c[1];
+            best.ms = t;
+        }
+        if (ctx->params.flags & CULDA_FLAG_VERBOSE)
+            fprintf(stderr, "culda: autotune G=%d blocks=%d grid=%d: %.3f ms\n", c[0], c[1], grid, t);
+    }
+    int32_t e = 0;
+    CK(cudaMemcpy(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (e) return fail(ctx, CULDA_ERR_DEVICE_STATE, "autotune: sampler reported device error 0x%x", e);
+    if (best.group_lanes == 0) return fail(ctx, CULDA_ERR_CUDA, "autotune: no sampler variant fits the device");
+    ctx->group_lanes = best.group_lanes;
+    ctx->sample_blocks = best.sample_blocks;
+    ctx->sample_grid = std::max(
+        1, std::min(ctx->num_items, num_sms(ctx->device) * sample_blocks_per_sm(ctx->K, best.group_lanes,
+                                                                                 best.sample_blocks)));
+    ctx->tuned = 1;
+    ctx->tune_ms = best.ms;
+    tune_store(key, best);
+    return CULDA_OK;
+}
+
 int build_graphs(culda_ctx *ctx) {
     for (int c = 0; c < 2; ++c) {
         if (ctx->graph[c]) {
@@ -212,11 +348,20 @@ int build_graphs(culda_ctx *ctx) {
     return CULDA_OK;
 }
 
-int pick_group_lanes(int requested) {
+int pick_group_lanes(int requested, int k) {
     if (requested == 1 || requested == 2 || requested == 4 || requested == 8 || requested == 16 || requested == 32)
         return requested;
-    return requested == 0 ? 8 : -1;
+    // measured on the 60M-token workload (K = 1024): 4 lanes per token with the
+    // 48-register budget is the fastest variant
+    return requested == 0 ? (k <= 2048 ? 4 : 8) : -1;
 }
+
+int pick_sample_blocks(int requested, int group_lanes, int k) {
+    if (requested != 0) return requested;
+    return (k <= 2048 && sample_variant_exists(group_lanes, kSampleBlocksHigh)) ? kSampleBlocksHigh
+                                                                              : kSampleBlocksDefault;
+}
+
 
 }  // namespace
 
@@ -395,8 +540,14 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: K=%d must be a multiple of 32 in [32, 4096]", p->k);
     if (!(p->alpha > 0.f) || !(p->beta > 0.f) || !std::isfinite(p->alpha) || !std::isfinite(p->beta))
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: alpha and beta must be positive");
-    const int gl = pick_group_lanes(p->group_lanes);
+    if ((p->flags & CULDA_FLAG_AUTOTUNE) && (p->group_lanes != 0 || p->sample_blocks != 0))
+        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: CULDA_FLAG_AUTOTUNE needs group_lanes = sample_blocks = 0");
+    const int gl = pick_group_lanes(p->group_lanes, p->k);
     if (gl < 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: group_lanes=%d", p->group_lanes);
+    const int sb = pick_sample_blocks(p->sample_blocks, gl, p->k);
+    if (!sample_variant_exists(gl, sb))
+        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: no sampler for group_lanes=%d sample_blocks=%d", gl,
+                    p->sample_blocks);
     if (c->num_docs <= 0 || c->num_words <= 0 || c->num_tokens <= 0 || !c->doc_ptr || !c->word_ptr || !c->doc_ids)
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: empty corpus");
     if (c->num_tokens >= (int64_t)INT32_MAX)
@@ -429,6 +580,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     ctx->K = p->k;
     ctx->N = c->num_tokens;
     ctx->group_lanes = gl;
+    ctx->sample_blocks = sb;
     int rc = CULDA_OK;
     auto bail = [&](int code) {
         culda_destroy(ctx);
@@ -588,7 +740,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
 
     // grids
     const int sms = num_sms(ctx->device);
-    int sbps = sample_blocks_per_sm(K, gl);
+    int sbps = sample_blocks_per_sm(K, gl, sb);
     if (sbps <= 0) {
         fail(ctx, CULDA_ERR_CUDA, "culda_create: sampler does not fit on the device for K=%d", K);
         return bail(CULDA_ERR_CUDA);
@@ -648,14 +800,26 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     ctx->cur = 0;
     rc = rebuild_counts(ctx);
     if (rc) return bail(rc);
+    if (p->flags & CULDA_FLAG_AUTOTUNE) {
+        // a cached result applies now; otherwise the variants are timed on the
+        // state after the first iterations, whose theta rows are shorter than
+        // the random initial ones and closer to the rest of the chain
+        TuneResult r;
+        if (tune_lookup(tune_key(ctx), r)) {
+            rc = autotune_sampler(ctx);
+            if (rc) return bail(rc);
+        } else {
+            ctx->tune_pending = true;
+        }
+    }
     rc = build_graphs(ctx);
     if (rc) return bail(rc);
     if (p->flags & CULDA_FLAG_VERBOSE)
         fprintf(stderr,
                 "culda: D=%d V=%d N=%lld K=%d items=%d hot_words=%d hot_items=%d item_tokens=%d theta_cap=%lld "
-                "sample_grid=%d theta_grid=%d G=%d\n",
+                "sample_grid=%d theta_grid=%d G=%d sample_blocks=%d\n",
                 D, V, (long long)N, K, ctx->num_items, ctx->num_hot, ctx->num_hot_items, ctx->item_tokens,
-                (long long)ctx->theta_cap, ctx->sample_grid, ctx->theta_grid, gl);
+                (long long)ctx->theta_cap, ctx->sample_grid, ctx->theta_grid, ctx->group_lanes, ctx->sample_blocks);
     *out = ctx;
     return CULDA_OK;
 #undef CKB
@@ -666,6 +830,13 @@ extern "C" int culda_iterate(culda_ctx *ctx, int n, culda_iter_stats *stats) {
     if (!ctx || n < 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_iterate: invalid argument");
     CK(cudaSetDevice(ctx->device));
     for (int i = 0; i < n; ++i) {
+        if (ctx->tune_pending && ctx->next_iteration >= kTuneIteration) {
+            ctx->tune_pending = false;
+            int rc = autotune_sampler(ctx);
+            if (rc) return rc;
+            rc = build_graphs(ctx);
+            if (rc) return rc;
+        }
         CK(cudaEventRecord(ctx->ev0, ctx->stream));
         if (ctx->graph[ctx->cur]) {
             CK(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
@@ -770,11 +941,9 @@ extern "C" int culda_get_theta(culda_ctx *ctx, int16_t *theta_a, int16_t *theta_
         CK(cudaMemcpyAsync(t.data(), ctx->d_theta, sizeof(ThetaEntry) * t.size(), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         for (size_t i = 0; i < t.size(); ++i) {
-            float cnt;
-            std::memcpy(&cnt, &t[i].x, sizeof(float));
             // the reference stores counts as int16 (thetaA): same truncation
-            if (theta_a) theta_a[i] = (int16_t)(uint16_t)(uint32_t)cnt;
-            if (theta_ja) theta_ja[i] = (int16_t)(uint16_t)(t[i].y >> 2);  // stored as 4 * topic
+            if (theta_a) theta_a[i] = (int16_t)(uint16_t)(t[i] & 0xFFFFu);
+            if (theta_ja) theta_ja[i] = (int16_t)(uint16_t)(t[i] >> 18);  // stored as 4 * topic
         }
     }
     if (max_ia) std::copy(ctx->h_max_ia.begin(), ctx->h_max_ia.end(), max_ia);
@@ -802,7 +971,8 @@ extern "C" int culda_sample_snapshot(culda_ctx *ctx, uint32_t iteration, uint16_
                            s));
     }
     CK(launch_uniforms(ctx->N, ctx->params.seed, nullptr, iteration, ctx->d_tok_index, ctx->d_u, s));
-    CK(launch_sample(sample_params(ctx, cur, iteration, nullptr), ctx->group_lanes, ctx->sample_grid, s));
+    CK(launch_sample(sample_params(ctx, cur, iteration, nullptr), ctx->group_lanes, ctx->sample_blocks,
+                     ctx->sample_grid, s));
     CK(launch_finalize_ll(ctx->d_item_ll, ctx->num_items, ctx->d_stats, nullptr, s));
     DevStats h{};
     int32_t e = 0;
@@ -856,6 +1026,9 @@ extern "C" int culda_get_info(const culda_ctx *ctx, culda_info *info) {
     info->item_tokens = ctx->item_tokens;
     info->group_lanes = ctx->group_lanes;
     info->sample_grid = ctx->sample_grid;
+    info->sample_blocks = ctx->sample_blocks;
+    info->tuned = ctx->tuned;
+    info->tune_ms = ctx->tune_ms;
     info->theta_grid = ctx->theta_grid;
     // hot_rows (when words are split), uniforms, sample, finalize_ll, theta_rebuild, copy_error
     info->kernels_per_iteration = (ctx->num_hot > 0 ? 1 : 0) + 5;

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
                 bits &= bits - 1u;
                 const uint32_t z = ((uint32_t)mi << 5) | (uint32_t)bit;
                 const uint32_t c = (cnt[z >> 1] >> ((z & 1u) << 4)) & 0xFFFFu;
-                theta[pos++] = make_uint2(__float_as_uint((float)c), z << 2);
+                theta[pos++] = theta_entry(z, c);
                 atomicAdd(&nk_acc[z], c);
             }
             __syncwarp();
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
         __syncwarp();
         const int new_end = start + ((nnz + 31) & ~31);
         const int zend = max(new_end, old_end);
-        for (int j = start + nnz + lane; j < zend; j += 32) theta[j] = make_uint2(0u, 0u);
+        for (int j = start + nnz + lane; j < zend; j += 32) theta[j] = 0u;
         if (lane == 0) {
             rows[d].y = new_end;
             my_rows += (e - b) * (int64_t)(new_end - start);
@@ -380,8 +380,8 @@ __global__ void __launch_bounds__(256) loglik_joint_kernel(int K, int V, int D, 
     for (int d = blockIdx.x; d < D; d += gridDim.x) {
         const int2 r = rows[d];
         for (int i = r.x + threadIdx.x; i < r.y; i += blockDim.x) {
-            const float cnt = __uint_as_float(theta[i].x);
-            if (cnt > 0.f) add(lgamma((double)cnt + alpha) - lg_a);
+            const uint32_t cnt = theta[i] & 0xFFFFu;
+            if (cnt > 0u) add(lgamma((double)cnt + alpha) - lg_a);
         }
         if (threadIdx.x == 0) add(-lgamma((double)(doc_ptr[d + 1] - doc_ptr[d]) + ka));
     }
@@ -558,10 +558,10 @@ extern "C" int culda_sample(const culda_sample_args *a, void *d_workspace, size_
     p.error = a->error ? a->error : counter + 1;
     int dev = 0;
     cudaGetDevice(&dev);
-    int bps = sample_blocks_per_sm(a->k, a->group_lanes);
+    int bps = sample_blocks_per_sm(a->k, a->group_lanes, kSampleBlocksDefault);
     if (bps <= 0) bps = 1;
     const int grid = std::max(1, std::min(a->num_items, num_sms(dev) * bps));
-    rc = cuda_status(launch_sample(p, a->group_lanes, grid, s));
+    rc = cuda_status(launch_sample(p, a->group_lanes, kSampleBlocksDefault, grid, s));
     if (rc) return rc;
     DevStats *st = (DevStats *)(counter + 8);
     rc = cuda_status(launch_finalize_ll(item_ll, a->num_items, st, nullptr, s));

@@ -8,10 +8,13 @@
 
 namespace culda {
 
-// One theta CSR entry: x = float bits of the count, y = 4 * topic (the byte
-// offset of the topic's phihat in the sampler's shared memory).  The sampler
-// then needs one shared-memory load and one multiply per entry.
-using ThetaEntry = uint2;
+// One theta CSR entry: the count (at most 65535, the longest doc) in the low
+// 16 bits and 4 * topic (the byte offset of the topic's phihat in the
+// sampler's shared memory; K <= 4096) in the high 16 bits.  Four bytes per
+// entry, like the reference's two int16 arrays, but read with one load.
+using ThetaEntry = uint32_t;
+
+__host__ __device__ inline uint32_t theta_entry(uint32_t topic, uint32_t count) { return (topic << 18) | count; }
 
 // Everything the sampler reads, passed by value.
 struct SampleParams {
@@ -61,8 +64,14 @@ inline int pow2_ceil(int k) {
 }
 
 size_t sample_smem_bytes(int k);
-int sample_blocks_per_sm(int k, int group_lanes);
-cudaError_t launch_sample(const SampleParams &p, int group_lanes, int grid, cudaStream_t s);
+// Sampler variants: lanes per token G and the register budget, given as the
+// resident CTAs per SM the kernel is compiled for (kSampleBlocksDefault for
+// every G; kSampleBlocksHigh for G = 4, 8, 16).
+constexpr int kSampleBlocksDefault = 8;
+constexpr int kSampleBlocksHigh = 10;
+bool sample_variant_exists(int group_lanes, int blocks_per_sm);
+int sample_blocks_per_sm(int k, int group_lanes, int blocks_per_sm);
+cudaError_t launch_sample(const SampleParams &p, int group_lanes, int blocks_per_sm, int grid, cudaStream_t s);
 
 size_t theta_smem_bytes(int k);
 int theta_blocks_per_sm(int k);

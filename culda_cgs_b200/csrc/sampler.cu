@@ -11,9 +11,10 @@
 // per step), keeping the running sum after every step in shared memory, and
 // then draws each token of the segment with its own Philox uniform.
 //
-// Theta entries are {float bits of the count, 4 * topic}: the product
-// theta_dk * phihat_wk is one shared-memory load at the entry's byte offset
-// and one multiply.
+// A theta entry is one 32-bit word: the count in the low 16 bits and 4 * topic
+// (the byte offset of the topic's phihat) in the high 16 bits.  The product
+// theta_dk * phihat_wk is one shared-memory load at that offset, an exact
+// integer-to-float conversion on the integer pipes and one multiply.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,12 +25,20 @@
 
 namespace culda {
 
+__device__ __forceinline__ uint32_t entry_count(uint32_t e) { return e & 0xFFFFu; }
+__device__ __forceinline__ int entry_topic(uint32_t e) { return (int)(e >> 18); }
+
+// The count as a float, exactly: 2^23 + c has c in its low mantissa bits.
+__device__ __forceinline__ float entry_count_f(uint32_t e) {
+    return __fsub_rn(__uint_as_float(0x4B000000u | (e & 0xFFFFu)), 8388608.0f);
+}
+
 // theta_dk * phihat_wk for one entry.  The explicit-rounding intrinsics keep
 // the compiler from fusing products and sums into different FMAs in the two
 // passes: both passes must produce bitwise the same sums.
-__device__ __forceinline__ float entry_prob(uint32_t count_bits, uint32_t byte_off, const float *ph) {
-    return __fmul_rn(__uint_as_float(count_bits), *reinterpret_cast<const float *>(
-                                                       reinterpret_cast<const char *>(ph) + byte_off));
+__device__ __forceinline__ float entry_prob(uint32_t e, const float *ph) {
+    return __fmul_rn(entry_count_f(e),
+                     *reinterpret_cast<const float *>(reinterpret_cast<const char *>(ph) + (e >> 16)));
 }
 
 __device__ __forceinline__ float fsum(float a, float b) { return __fadd_rn(a, b); }
@@ -106,11 +115,9 @@ __device__ __forceinline__ int dense_bucket_search(const float *qc, int K, float
 }
 
 // ------------------------------------------------------------- row walk
-// Theta entries per lane per step (8 bytes each, loaded 16 bytes at a time).
-// Four keeps the sampler under 64 registers; eight needs about 80 and loses
-// occupancy for no gain on the 60M-token workload.
+// Theta entries per lane per step: one 16-byte load.  A group of 8 lanes
+// then reads one 128-byte line of a row per step (rows start on 32 entries).
 constexpr int kLaneEntries = 4;
-constexpr int kLaneVecs = kLaneEntries / 2;
 
 template <int G>
 struct SampleShape {
@@ -121,28 +128,27 @@ struct SampleShape {
 };
 
 struct Step {
-    uint4 v[kLaneVecs];  // v[j] = {count 2j, offset 2j, count 2j+1, offset 2j+1}
+    uint32_t e[kLaneEntries];
 };
 
 __device__ __forceinline__ Step load_step(const ThetaEntry *__restrict__ theta, int idx, int re) {
     Step st;
     if (idx < re) {  // rows end on a multiple of 32 entries, idx on a multiple of kLaneEntries
-        const uint4 *p = reinterpret_cast<const uint4 *>(theta + idx);
-#pragma unroll
-        for (int j = 0; j < kLaneVecs; ++j) st.v[j] = __ldg(p + j);
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(theta + idx));
+        st.e[0] = v.x;
+        st.e[1] = v.y;
+        st.e[2] = v.z;
+        st.e[3] = v.w;
     } else {
 #pragma unroll
-        for (int j = 0; j < kLaneVecs; ++j) st.v[j] = make_uint4(0u, 0u, 0u, 0u);
+        for (int j = 0; j < kLaneEntries; ++j) st.e[j] = 0u;
     }
     return st;
 }
 
 __device__ __forceinline__ void step_probs(const Step &st, const float *ph, float p[kLaneEntries]) {
 #pragma unroll
-    for (int j = 0; j < kLaneVecs; ++j) {
-        p[2 * j] = entry_prob(st.v[j].x, st.v[j].y, ph);
-        p[2 * j + 1] = entry_prob(st.v[j].z, st.v[j].w, ph);
-    }
+    for (int j = 0; j < kLaneEntries; ++j) p[j] = entry_prob(st.e[j], ph);
 }
 
 // Pairwise sum of the lane's entries.
@@ -162,10 +168,8 @@ template <int G>
 __device__ __forceinline__ int step_last_nonzero(const Step &st, unsigned m, int lane) {
     int last = -1;
 #pragma unroll
-    for (int j = 0; j < kLaneVecs; ++j) {
-        if (st.v[j].x) last = (int)(st.v[j].y >> 2);
-        if (st.v[j].z) last = (int)(st.v[j].w >> 2);
-    }
+    for (int j = 0; j < kLaneEntries; ++j)
+        if (entry_count(st.e[j])) last = entry_topic(st.e[j]);
     const unsigned nb = group_ballot<G>(last >= 0, m, lane);
     return nb ? group_bcast<G>(last, 31 - __clz(nb), m) : -1;
 }
@@ -183,9 +187,7 @@ __device__ __forceinline__ int resolve_step(const Step &st, float base, float T,
 #pragma unroll
     for (int i = 0; i < kLaneEntries; ++i) {
         cum += p[i];
-        const uint32_t cnt = (i & 1) ? st.v[i >> 1].z : st.v[i >> 1].x;
-        const uint32_t off = (i & 1) ? st.v[i >> 1].w : st.v[i >> 1].y;
-        if (hit < 0 && cnt && cum > T) hit = (int)(off >> 2);
+        if (hit < 0 && entry_count(st.e[i]) && cum > T) hit = entry_topic(st.e[i]);
     }
     const unsigned hb = group_ballot<G>(hit >= 0, m, lane);
     if (hb) return group_bcast<G>(hit, __ffs(hb) - 1, m);
@@ -203,12 +205,16 @@ __device__ __forceinline__ float row_sum(const ThetaEntry *__restrict__ theta, c
     __syncwarp(m);  // the group's previous row is no longer being read from pref
     float s = 0.f, c = 0.f;
     int nst = 0;
+    // the next step's entries are loaded before this step is reduced, so two
+    // row loads per lane are in flight
+    Step st = load_step(theta, rs + kLaneEntries * gl, re);
     for (int base = rs; base < re; base += kStep, ++nst) {
-        const Step st = load_step(theta, base + kLaneEntries * gl, re);
+        const Step nx = load_step(theta, base + kStep + kLaneEntries * gl, re);
         float p[kLaneEntries];
         step_probs(st, ph, p);
         neumaier(s, c, group_sum<G>(lane_sum(p), m));
         if (gl == 0 && nst < kMax) pref[nst] = s + c;
+        st = nx;
     }
     __syncwarp(m);  // pref is complete before any lane searches it
     nst_out = nst;
@@ -254,14 +260,17 @@ __device__ __forceinline__ int draw_topic(const ThetaEntry *__restrict__ theta, 
     int last = -1;
     for (int i = max(rs, re - 32); i < re; ++i) {
         const ThetaEntry e = __ldg(theta + i);
-        if (e.x) last = (int)(e.y >> 2);
+        if (entry_count(e)) last = entry_topic(e);
     }
     return last;
 }
 
 // -------------------------------------------------------------- the kernel
-template <int G>
-__global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleParams p) {
+// MINB resident CTAs per SM is the register budget the compiler is held to:
+// 8 -> at most 64 registers (32 warps per SM), 10 -> at most 48 (40 warps),
+// with a few spills.
+template <int G, int MINB>
+__global__ void __launch_bounds__(kSampleThreads, MINB) sample_kernel(const SampleParams p) {
     extern __shared__ float smem[];
     using Shape = SampleShape<G>;
     const int K = p.k, KP = p.kmask + 1;
@@ -413,25 +422,36 @@ size_t sample_smem_bytes(int k) {
     return ((size_t)2 * k + (size_t)pow2_ceil(k) + (size_t)SampleShape<1>::kPrefixFloats) * sizeof(float);
 }
 
-template <int G>
+template <int G, int MINB>
 static const void *sample_fn() {
-    return reinterpret_cast<const void *>(&sample_kernel<G>);
+    return reinterpret_cast<const void *>(&sample_kernel<G, MINB>);
 }
 
-static const void *sample_kernel_for(int g) {
-    switch (g) {
-        case 1: return sample_fn<1>();
-        case 2: return sample_fn<2>();
-        case 4: return sample_fn<4>();
-        case 8: return sample_fn<8>();
-        case 16: return sample_fn<16>();
-        case 32: return sample_fn<32>();
-        default: return nullptr;
-    }
+static const void *sample_kernel_for(int g, int minb) {
+    if (minb == kSampleBlocksDefault) switch (g) {
+            case 1: return sample_fn<1, kSampleBlocksDefault>();
+            case 2: return sample_fn<2, kSampleBlocksDefault>();
+            case 4: return sample_fn<4, kSampleBlocksDefault>();
+            case 8: return sample_fn<8, kSampleBlocksDefault>();
+            case 16: return sample_fn<16, kSampleBlocksDefault>();
+            case 32: return sample_fn<32, kSampleBlocksDefault>();
+            default: return nullptr;
+        }
+    if (minb == kSampleBlocksHigh) switch (g) {
+            case 4: return sample_fn<4, kSampleBlocksHigh>();
+            case 8: return sample_fn<8, kSampleBlocksHigh>();
+            case 16: return sample_fn<16, kSampleBlocksHigh>();
+            default: return nullptr;
+        }
+    return nullptr;
 }
 
-int sample_blocks_per_sm(int k, int group_lanes) {
-    const void *fn = sample_kernel_for(group_lanes);
+bool sample_variant_exists(int group_lanes, int blocks_per_sm) {
+    return sample_kernel_for(group_lanes, blocks_per_sm) != nullptr;
+}
+
+int sample_blocks_per_sm(int k, int group_lanes, int blocks_per_sm) {
+    const void *fn = sample_kernel_for(group_lanes, blocks_per_sm);
     if (!fn) return 0;
     const size_t smem = sample_smem_bytes(k);
     if (allow_smem(fn, smem, nullptr) != cudaSuccess) return 0;
@@ -440,10 +460,10 @@ int sample_blocks_per_sm(int k, int group_lanes) {
     return n;
 }
 
-cudaError_t launch_sample(const SampleParams &p, int group_lanes, int grid, cudaStream_t s) {
+cudaError_t launch_sample(const SampleParams &p, int group_lanes, int blocks_per_sm, int grid, cudaStream_t s) {
     const size_t smem = sample_smem_bytes(p.k);
     void *args[] = {const_cast<SampleParams *>(&p)};
-    const void *fn = sample_kernel_for(group_lanes);
+    const void *fn = sample_kernel_for(group_lanes, blocks_per_sm);
     if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = allow_smem(fn, smem, s);
     if (e != cudaSuccess) return e;
@@ -525,7 +545,7 @@ __global__ void check_theta_kernel(int num_docs, int K, const int2 *__restrict__
         }
         for (int i = r.x + lane; i < r.y; i += 32) {
             const ThetaEntry e = theta[i];
-            if ((e.y & 3u) || (e.y >> 2) >= (uint32_t)K) atomicOr(error, kErrTopicRange);
+            if ((e & 0x30000u) || (e >> 18) >= (uint32_t)K) atomicOr(error, kErrTopicRange);
         }
     }
 }

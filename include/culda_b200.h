@@ -27,13 +27,13 @@
  *   doc_ptr   int64[D+1]  token count prefix per doc (reference: docRevIndices)
  *   doc_tok   int32[N]    word-major token index of every token, grouped by doc
  *                         and ascending within a doc (reference: docRevIdx)
- *   theta     uint32[2*cap] CSR entries of two words: {float bits of the
- *                         count, 4 * topic}, ascending topic inside a row, zero
- *                         padded (reference: thetaA and thetaJA, two int16
- *                         arrays, lda_theta_kernel.cu:55-58).  The count is kept
- *                         as a float and the topic as a byte offset so the
- *                         sampler needs one shared-memory load and one multiply
- *                         per entry.
+ *   theta     uint32[cap] CSR entries, one word each: the count in the low
+ *                         16 bits, 4 * topic in the high 16 bits; ascending
+ *                         topic inside a row, zero padded (reference: thetaA
+ *                         and thetaJA, two int16 arrays,
+ *                         lda_theta_kernel.cu:55-58).  The topic is kept as a
+ *                         byte offset so the sampler needs one 16-byte load per
+ *                         four entries and one shared-memory load per entry.
  *   theta_rows int32[2*D] {row start, row end} per doc; start is the reference's
  *                         thetaMaxIA[d], end its thetaCurIA[d] = start + roundup32(nnz)
  *   nk        int32[K]    tokens per topic (reference: phiTopic)
@@ -148,12 +148,20 @@ typedef struct culda_params {
     int32_t group_lanes;  /* lanes per token in the sampler: 0 = auto, else 1,2,4,8,16,32 */
     int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto */
     int32_t flags;        /* CULDA_FLAG_* */
+    int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (8),
+                              8 (<= 64 registers), or 10 (<= 48 registers; group_lanes 4, 8, 16) */
 } culda_params;
 
 enum {
     CULDA_FLAG_NO_GRAPH = 1,      /* launch the iteration kernel by kernel instead of one CUDA graph */
     CULDA_FLAG_VERBOSE = 2,       /* print set-up details to stderr */
-    CULDA_FLAG_NO_REORDER = 4     /* keep tokens in input order inside each word (default: by doc length) */
+    CULDA_FLAG_NO_REORDER = 4,    /* keep tokens in input order inside each word (default: by doc length) */
+    CULDA_FLAG_AUTOTUNE = 8       /* time the sampler variants (lanes per token x register budget) on the
+                                     state before iteration 3 (after two iterations with the default
+                                     variant) and keep the fastest; group_lanes and sample_blocks must be
+                                     0.  Results are cached per (device name, N, D, V, K) in the process
+                                     and, when the environment variable CULDA_TUNE_CACHE names a file, in
+                                     that file; a cached result applies from the first iteration. */
 };
 
 typedef struct culda_iter_stats {
@@ -216,11 +224,15 @@ typedef struct culda_info {
     int32_t item_tokens;        /* largest item */
     int32_t group_lanes;        /* lanes per token in the sampler */
     int32_t sample_grid;        /* persistent sampler CTAs */
+    int32_t sample_blocks;      /* the sampler's register budget (resident CTAs per SM) */
     int32_t theta_grid;         /* theta rebuild CTAs */
     int32_t kernels_per_iteration;
     int64_t theta_capacity;     /* theta entries */
     int64_t device_bytes;       /* device memory held by the context */
     double doc_term;            /* sum_d L_d log(L_d + K alpha) */
+    int32_t tuned;              /* sampler variant: 0 = given or default (or tuning still pending),
+                                   1 = timed, 2 = from the tuning cache */
+    float tune_ms;              /* the chosen variant's sampler time when it was timed (tuned != 0) */
 } culda_info;
 
 int culda_get_info(const culda_ctx *ctx, culda_info *info);

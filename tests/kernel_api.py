@@ -82,7 +82,7 @@ def prepare(corpus: cb.Corpus, k: int, alpha: float, beta: float, z: np.ndarray,
         "word_ptr": dev(wp.astype(np.int64)), "doc_ptr": dev(dp.astype(np.int64)), "doc_ids": dev(idc),
         "doc_tok": dev(corpus.doc_tokens()), "z": dev(z.astype(np.uint16)),
         "z_out": torch.zeros(len(ids), dtype=torch.int16, device="cuda"),
-        "rows": dev(rows), "theta": torch.zeros(2 * cap, dtype=torch.int32, device="cuda"),
+        "rows": dev(rows), "theta": torch.zeros(cap, dtype=torch.int32, device="cuda"),
         "nk": torch.zeros(k, dtype=torch.int32, device="cuda"),
         "stats": torch.zeros(3, dtype=torch.int64, device="cuda"),
         "items": dev(np.frombuffer(bytes(items), dtype=np.uint8)),

@@ -42,13 +42,14 @@ def test_version_and_status_strings():
 
 
 def _params(**kw):
-    d = dict(k=64, alpha=0.1, beta=0.01, seed=1, device=0, group_lanes=0, item_tokens=0, flags=0)
+    d = dict(k=64, alpha=0.1, beta=0.01, seed=1, device=0, group_lanes=0, item_tokens=0, flags=0, sample_blocks=0)
     d.update(kw)
     return _ffi.Params(**d)
 
 
 @pytest.mark.parametrize("kw", [dict(k=48), dict(k=0), dict(k=8192), dict(alpha=0.0), dict(beta=-1.0),
-                                dict(group_lanes=3)])
+                                dict(group_lanes=3), dict(sample_blocks=9), dict(group_lanes=1, sample_blocks=10),
+                                dict(group_lanes=8, flags=_ffi.CULDA_FLAG_AUTOTUNE)])
 def test_create_rejects_bad_params(kw):
     c = cb.Corpus.generate(TINY.gen)
     ctx = C.c_void_p()

@@ -65,11 +65,10 @@ def test_update_theta(problem):
     p, s = problem
     assert update_theta(p) == 0
     torch.cuda.synchronize()
-    t = host(p.d["theta"], np.uint32).reshape(-1, 2)
-    counts = t[:, 0].view(np.float32)
-    assert np.array_equal(counts.astype(np.int64).astype(np.int16), s.theta_a)
-    assert np.array_equal((t[:, 1] >> 2).astype(np.int16), s.theta_ja)
-    assert ((t[:, 1] & 3) == 0).all()
+    t = host(p.d["theta"], np.uint32)
+    assert np.array_equal((t & 0xFFFF).astype(np.int16), s.theta_a)
+    assert np.array_equal((t >> 18).astype(np.int16), s.theta_ja)
+    assert ((t >> 16) & 3 == 0).all()
     rows = host(p.d["rows"], np.int32).reshape(-1, 2)
     assert np.array_equal(rows[:, 0], s.max_ia[:-1]) and np.array_equal(rows[:, 1], s.cur_ia)
     assert np.array_equal(host(p.d["nk"], np.int32), s.nk)
@@ -108,8 +107,7 @@ def test_sample_rejects_out_of_range_theta(problem):
     p, s = problem
     assert update_theta(p) == 0
     theta = p.d["theta"].clone()
-    bad = theta.view(-1, 2)
-    bad[0, 1] = 4 * p.k  # topic K: one past the last valid topic
+    theta[0] = (p.k << 18) | 1  # topic K: one past the last valid topic
     lib = cb.lib()
     a = sample_args(p, seed=1, iteration=1)
     a.theta = ptr(theta)

@@ -54,16 +54,20 @@ def assert_draws_match(z_gpu, z_ora, margin, check_rate=True):
         assert (z_gpu != z_ora).mean() < 1e-3
 
 
-CASES = [
-    ("tiny-k64-g8", TINY.gen, 64, 8, 0),
-    ("tiny-k64-g1-hot", TINY.gen, 64, 1, 64),
-    ("tiny-k32-g2", TINY.gen, 32, 2, 0),
-    ("mini-k1024-g4", MINI.gen, 1024, 4, 0),
-    ("mini-k1024-g8-hot", MINI.gen, 1024, 8, 300),
-    ("mini-k1024-g16", MINI.gen, 1024, 16, 0),
-    ("mini-k1024-g32", MINI.gen, 1024, 32, 0),
-    ("mini-k256-g1", MINI.gen, 256, 1, 0),
-    ("mini-k4096-g8", MINI.gen, 4096, 8, 0),
+CASES = [  # name, corpus, K, lanes per token, item tokens (0 = auto), sampler register budget (0 = auto)
+    ("tiny-k64-g8", TINY.gen, 64, 8, 0, 0),
+    ("tiny-k64-g1-hot", TINY.gen, 64, 1, 64, 0),
+    ("tiny-k32-g2", TINY.gen, 32, 2, 0, 0),
+    ("mini-k1024-g4", MINI.gen, 1024, 4, 0, 0),
+    ("mini-k1024-g8-hot", MINI.gen, 1024, 8, 300, 0),
+    ("mini-k1024-g16", MINI.gen, 1024, 16, 0, 0),
+    ("mini-k1024-g32", MINI.gen, 1024, 32, 0, 0),
+    ("mini-k256-g1", MINI.gen, 256, 1, 0, 0),
+    ("mini-k4096-g8", MINI.gen, 4096, 8, 0, 0),
+    ("mini-k1024-g8-b10", MINI.gen, 1024, 8, 0, 10),
+    ("mini-k1024-g4-b10-hot", MINI.gen, 1024, 4, 300, 10),
+    ("mini-k1024-g16-b10", MINI.gen, 1024, 16, 0, 10),
+    ("tiny-k64-g8-b10", TINY.gen, 64, 8, 0, 10),
 ]
 
 
@@ -72,11 +76,14 @@ def corpora():
     return {id(g): cb.Corpus.generate(g) for g in (TINY.gen, MINI.gen)}
 
 
-@pytest.mark.parametrize("name,gen,k,g,item_tokens", CASES, ids=[c[0] for c in CASES])
-def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens):
+@pytest.mark.parametrize("name,gen,k,g,item_tokens,blocks", CASES, ids=[c[0] for c in CASES])
+def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens, blocks):
     c = corpora[id(gen)]
     seed = 1234
-    with cb.LDA(c, k, 50.0 / 1024, 0.01, seed=seed, group_lanes=g, item_tokens=item_tokens) as m:
+    with cb.LDA(c, k, 50.0 / 1024, 0.01, seed=seed, group_lanes=g, item_tokens=item_tokens,
+                sample_blocks=blocks) as m:
+        default_blocks = 10 if (k <= 2048 and g in (4, 8, 16)) else 8
+        assert m.info()["sample_blocks"] == (blocks or default_blocks)
         z0 = m.topics()
         assert np.array_equal(z0, O.init_topics(c.num_tokens, k, seed))
         s0 = assert_counts_exact(m, c)
@@ -102,14 +109,14 @@ def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens):
         assert np.array_equal(m.topics(), s.z)
 
 
-@pytest.mark.parametrize("g", [1, 4, 8, 32])
-def test_long_chain_keeps_device_state_consistent(g):
-    """~10M draws per lane width: tokens whose target lands within a rounding of
-    a bucket boundary must still get a topic (the sampler's error word stays 0)."""
+@pytest.mark.parametrize("g,blocks", [(1, 8), (4, 8), (8, 8), (32, 8), (8, 10)])
+def test_long_chain_keeps_device_state_consistent(g, blocks):
+    """~10M draws per sampler variant: tokens whose target lands within a rounding
+    of a bucket boundary must still get a topic (the sampler's error word stays 0)."""
     from culda_cgs_b200.configs import SMALL
 
     c = cb.Corpus.generate(SMALL.gen)
-    with cb.LDA(c, 1024, 50.0 / 1024, 0.01, seed=21 + g, group_lanes=g) as m:
+    with cb.LDA(c, 1024, 50.0 / 1024, 0.01, seed=21 + g, group_lanes=g, sample_blocks=blocks) as m:
         stats = m.iterate(10)
         assert all(s["status"] == 0 for s in stats)
         assert stats[-1]["loglik"] > stats[0]["loglik"]

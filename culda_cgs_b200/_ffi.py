@@ -76,6 +76,16 @@ class SampleArgs(C.Structure):
 
 
 # every symbol the header declares, with its signature
+CULDA_GEMM_F32, CULDA_GEMM_BIAS_GELU, CULDA_GEMM_GELU_BWD = 0, 1, 2
+
+
+class GemmArgs(C.Structure):
+    _fields_ = [("m", i32), ("n", i32), ("k", i32), ("a", C.c_void_p), ("lda", i32), ("b", C.c_void_p),
+                ("ldb", i32), ("epilogue", i32), ("alpha", f32), ("out_f32", C.c_void_p), ("out_bf16", C.c_void_p),
+                ("out_bf16_t", C.c_void_p), ("ldo", i32), ("ld_t", i32), ("bias", C.c_void_p), ("pre", C.c_void_p),
+                ("colsum", C.c_void_p), ("error", C.c_void_p)]
+
+
 SIGNATURES = {
     "culda_status_string": (C.c_char_p, [C.c_int]),
     "culda_version": (C.c_char_p, []),
@@ -109,6 +119,7 @@ SIGNATURES = {
     "culda_sample": (C.c_int, [P(SampleArgs), C.c_void_p, C.c_size_t, C.c_void_p]),
     "culda_sample_noalloc": (C.c_int, [P(SampleArgs), C.c_void_p]),
     "culda_loglik": (C.c_int, [C.c_void_p, f64, i64, P(f64), C.c_void_p]),
+    "culda_gemm_bf16": (C.c_int, [P(GemmArgs), C.c_void_p]),
 }
 
 _lib = None

@@ -19,7 +19,9 @@ enum : int32_t {
     kErrTopicRange = 1,   // a topic >= K was found in the topic array
     kErrDocRange = 2,     // a doc id outside [0, D) reached the sampler
     kErrRowRange = 4,     // a theta row outside the theta array or misaligned
-    kErrLongDoc = 8       // a document longer than 65535 tokens
+    kErrLongDoc = 8,      // a document longer than 65535 tokens
+    kErrTimeout = 16,     // a bounded wait on an mbarrier gave up (the tile was not stored)
+    kErrWordRange = 32    // a word id outside [0, V) reached the encoder
 };
 
 // Sampler block size and the dynamic shared memory it needs for K topics.

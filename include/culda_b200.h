@@ -365,6 +365,42 @@ int culda_sample_noalloc(const culda_sample_args *a, void *stream);
  * host (synchronises the stream). */
 int culda_loglik(const double *d_loglik_sum, double doc_term, int64_t num_tokens, double *loglik, void *stream);
 
+/* ------------------------------------------- tensor-core GEMM (no reference counterpart)
+ * The BF16 GEMM the document encoder is built from: C = A * B^T with A
+ * [m x k] and B [n x k] row-major BF16 (k contiguous), FP32 accumulation on the
+ * tensor cores, and one of the encoder's fused epilogues:
+ *   CULDA_GEMM_F32        out_f32[m x n] = alpha * C (+ bias[col] when bias != NULL)
+ *   CULDA_GEMM_BIAS_GELU  out_f32 = C + bias (the pre-activation);
+ *                         out_bf16[m x n] and out_bf16_t[n x m] = GELU(C + bias)
+ *   CULDA_GEMM_GELU_BWD   g = C * GELU'(pre[m x n]); out_bf16 and out_bf16_t = g;
+ *                         colsum[col] += sum over rows of g (when colsum != NULL)
+ * GELU is x * Phi(x) (the error-function form).  m and n must be multiples of
+ * 128, k of 64; lda, ldb multiples of 8 elements; row-major outputs use row
+ * stride ldo, the transposed output ld_t.  A device error word (optional)
+ * receives bit 16 if a bounded wait inside the kernel gave up. */
+enum { CULDA_GEMM_F32 = 0, CULDA_GEMM_BIAS_GELU = 1, CULDA_GEMM_GELU_BWD = 2 };
+
+typedef struct culda_gemm_args {
+    int32_t m, n, k;
+    const void *a;      /* bf16 [m x lda] */
+    int32_t lda;
+    const void *b;      /* bf16 [n x ldb] */
+    int32_t ldb;
+    int32_t epilogue;   /* CULDA_GEMM_* */
+    float alpha;        /* CULDA_GEMM_F32 scale */
+    float *out_f32;     /* [m x ldo] */
+    void *out_bf16;     /* bf16 [m x ldo] */
+    void *out_bf16_t;   /* bf16 [n x ld_t] */
+    int32_t ldo;
+    int32_t ld_t;
+    const float *bias;  /* [n] */
+    const float *pre;   /* [m x ldo] */
+    float *colsum;      /* [n] */
+    int32_t *error;     /* device int32 or NULL */
+} culda_gemm_args;
+
+int culda_gemm_bf16(const culda_gemm_args *a, void *stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -86,6 +86,16 @@ class GemmArgs(C.Structure):
                 ("colsum", C.c_void_p), ("error", C.c_void_p)]
 
 
+CULDA_ENC_EMBED, CULDA_ENC_HIDDEN = 256, 512
+CULDA_ENC_E, CULDA_ENC_W1, CULDA_ENC_B1, CULDA_ENC_W2, CULDA_ENC_B2, CULDA_ENC_W3, CULDA_ENC_B3 = range(7)
+CULDA_ENC_GRAD = 16
+
+
+class EncoderParams(C.Structure):
+    _fields_ = [("num_words", i32), ("k", i32), ("max_batch", i32), ("device", i32), ("seed", u64), ("lr", f32),
+                ("beta1", f32), ("beta2", f32), ("eps", f32)]
+
+
 SIGNATURES = {
     "culda_status_string": (C.c_char_p, [C.c_int]),
     "culda_version": (C.c_char_p, []),
@@ -120,6 +130,17 @@ SIGNATURES = {
     "culda_sample_noalloc": (C.c_int, [P(SampleArgs), C.c_void_p]),
     "culda_loglik": (C.c_int, [C.c_void_p, f64, i64, P(f64), C.c_void_p]),
     "culda_gemm_bf16": (C.c_int, [P(GemmArgs), C.c_void_p]),
+    "culda_encoder_create": (C.c_int, [P(EncoderParams), P(C.c_void_p)]),
+    "culda_encoder_destroy": (C.c_int, [C.c_void_p]),
+    "culda_encoder_tensor_size": (i64, [C.c_void_p, i32]),
+    "culda_encoder_get_tensor": (C.c_int, [C.c_void_p, i32, C.c_void_p]),
+    "culda_encoder_set_tensor": (C.c_int, [C.c_void_p, i32, C.c_void_p]),
+    "culda_encoder_forward": (C.c_int, [C.c_void_p, i32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "culda_encoder_backward": (C.c_int, [C.c_void_p, i32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(f64),
+                                         C.c_void_p]),
+    "culda_encoder_train_step": (C.c_int, [C.c_void_p, i32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           P(f64), C.c_void_p]),
 }
 
 _lib = None

@@ -1,0 +1,34 @@
+// encoder.cuh — internal interface of the document encoder (encoder.cu) for
+// the context-level training and proposal code.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/culda_b200.h"
+
+namespace culda {
+
+// Where the cross-entropy target of batch row b comes from: a dense
+// [batch x K] array, or the doc's accumulated topic counts acc[d*K + k]
+// (summed over n snapshots) as (acc * inv_n + alpha) / (L_d + K alpha).
+struct EncoderTarget {
+    const float *dense = nullptr;
+    const float *acc = nullptr;
+    float inv_n = 1.0f;
+    float alpha = 0.0f;
+};
+
+// One forward (+ backward, + Adam step) pass; probs (optional) receives q.
+// Returns a CULDA status; the loss is summed on the device into *d_loss.
+int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t *doc_ptr, const int32_t *words,
+                 const EncoderTarget *target, bool update, float *probs, cudaStream_t s);
+
+// Mean cross-entropy of the passes since the last call (synchronises s).
+int encoder_take_loss(culda_encoder *e, int batch_rows, double *loss, cudaStream_t s);
+
+int encoder_k(const culda_encoder *e);
+int encoder_max_batch(const culda_encoder *e);
+int32_t *encoder_error_word(culda_encoder *e);
+
+}  // namespace culda

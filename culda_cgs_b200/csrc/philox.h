@@ -55,7 +55,22 @@ CULDA_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
 
 // Counter layout used everywhere in this library:
 //   {token index low, token index high, iteration, purpose}
-enum : uint32_t { kPurposeSample = 0u, kPurposeInit = 1u, kPurposeProposal = 2u, kPurposeAccept = 3u };
+// The counter's last word: one independent stream per use.
+enum : uint32_t {
+    kPurposeSample = 0u,    // plain CGS draw
+    kPurposeInit = 1u,      // initial topics
+    kPurposeProposal = 2u,  // Metropolis-Hastings proposals and acceptances
+    kPurposeAccept = 3u,
+    kPurposeWeights = 4u,   // encoder weight initialisation
+    kPurposeShuffle = 5u,   // encoder training batch order
+    kPurposeWarm = 6u       // encoder warm start of new documents' topics
+};
+
+// All four words of one Philox block.
+CULDA_HD u32x4 philox_token4(uint64_t seed, uint64_t token, uint32_t iteration, uint32_t purpose) {
+    u32x4 c = {(uint32_t)token, (uint32_t)(token >> 32), iteration, purpose};
+    return philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
 
 CULDA_HD uint32_t philox_token(uint64_t seed, uint64_t token, uint32_t iteration, uint32_t purpose) {
     u32x4 c = {(uint32_t)token, (uint32_t)(token >> 32), iteration, purpose};

@@ -401,6 +401,62 @@ typedef struct culda_gemm_args {
 
 int culda_gemm_bf16(const culda_gemm_args *a, void *stream);
 
+/* ------------------------------- document encoder (no reference counterpart)
+ * A small network that maps a document's bag of words to a distribution over
+ * the K topics, used as an independent Metropolis-Hastings proposal and to
+ * warm-start topics of new documents:
+ *   x0 = mean over the doc's tokens of E[word]         E: [V x 256]
+ *   h1 = GELU(W1 x0 + b1), h2 = GELU(W2 h1 + b2)       W1: [512 x 256], W2: [512 x 512]
+ *   q  = softmax(W3 h2 + b3)                           W3: [K x 512]
+ * BF16 operands on the tensor cores (culda_gemm_bf16) with FP32 accumulation
+ * and FP32 master weights; trained with Adam on the cross-entropy
+ * -sum_k target_k log q_k, averaged over the batch.
+ * Batches are CSR slices: doc b of a batch is docs[b] (or b when docs is
+ * NULL) of the CSR (doc_ptr int64[], words int32[] word ids), all device
+ * pointers. */
+#define CULDA_ENC_EMBED 256
+#define CULDA_ENC_HIDDEN 512
+
+typedef struct culda_encoder culda_encoder;
+
+typedef struct culda_encoder_params {
+    int32_t num_words;   /* V */
+    int32_t k;           /* topics: a multiple of 128, up to 4096 */
+    int32_t max_batch;   /* docs per call, 1..65536 (rounded up to 128 inside) */
+    int32_t device;
+    uint64_t seed;       /* Philox key of the initial weights */
+    float lr;            /* Adam step size (0 = 1e-3) */
+    float beta1, beta2;  /* Adam decay rates (0 = 0.9, 0.999) */
+    float eps;           /* Adam epsilon (0 = 1e-8) */
+} culda_encoder_params;
+
+/* Tensors of the encoder, for culda_encoder_get/set_tensor (FP32, row-major). */
+enum {
+    CULDA_ENC_E = 0, CULDA_ENC_W1 = 1, CULDA_ENC_B1 = 2, CULDA_ENC_W2 = 3, CULDA_ENC_B2 = 4, CULDA_ENC_W3 = 5,
+    CULDA_ENC_B3 = 6,
+    CULDA_ENC_GRAD = 16  /* + tensor: its gradient from the last backward pass */
+};
+
+int culda_encoder_create(const culda_encoder_params *p, culda_encoder **out);
+int culda_encoder_destroy(culda_encoder *e);
+int64_t culda_encoder_tensor_size(const culda_encoder *e, int32_t which);  /* elements, < 0 if unknown */
+int culda_encoder_get_tensor(culda_encoder *e, int32_t which, float *host);
+int culda_encoder_set_tensor(culda_encoder *e, int32_t which, const float *host);  /* weights only */
+
+/* q for a batch: d_probs [batch x K] FP32 (device). */
+int culda_encoder_forward(culda_encoder *e, int32_t batch, const int32_t *d_docs, const int64_t *d_doc_ptr,
+                          const int32_t *d_words, float *d_probs, void *stream);
+
+/* Forward and backward against d_target [batch x K] (device, rows summing to
+ * 1): leaves the gradients in the encoder (CULDA_ENC_GRAD + tensor) and the
+ * mean cross-entropy in *loss (host; synchronises the stream). */
+int culda_encoder_backward(culda_encoder *e, int32_t batch, const int32_t *d_docs, const int64_t *d_doc_ptr,
+                           const int32_t *d_words, const float *d_target, double *loss, void *stream);
+
+/* culda_encoder_backward followed by one Adam step on every weight. */
+int culda_encoder_train_step(culda_encoder *e, int32_t batch, const int32_t *d_docs, const int64_t *d_doc_ptr,
+                             const int32_t *d_words, const float *d_target, double *loss, void *stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -48,7 +48,7 @@ class Params(C.Structure):
 class IterStats(C.Structure):
     _fields_ = [("iteration", i32), ("status", i32), ("seconds", f64), ("loglik", f64), ("tokens_per_sec", f64),
                 ("row_entries", i64), ("theta_nnz", i64), ("token_nnz", i64), ("sample_seconds", f64),
-                ("rebuild_seconds", f64)]
+                ("rebuild_seconds", f64), ("accept_rate", f64)]
 
 
 class Info(C.Structure):
@@ -141,6 +141,15 @@ SIGNATURES = {
                                          C.c_void_p]),
     "culda_encoder_train_step": (C.c_int, [C.c_void_p, i32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            P(f64), C.c_void_p]),
+    "culda_accumulate_theta": (C.c_int, [C.c_void_p]),
+    "culda_train_encoder": (C.c_int, [C.c_void_p, C.c_void_p, i32, u64, P(f64)]),
+    "culda_encoder_init_from_phi": (C.c_int, [C.c_void_p, C.c_void_p, u64]),
+    "culda_set_proposal": (C.c_int, [C.c_void_p, C.c_void_p, f32]),
+    "culda_get_proposal": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "culda_iterate_mh": (C.c_int, [C.c_void_p, i32, i32, P(IterStats)]),
+    "culda_mh_snapshot": (C.c_int, [C.c_void_p, u32, i32, C.c_void_p]),
+    "culda_set_frozen_phi": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "culda_warm_start": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None

@@ -87,6 +87,26 @@ class Corpus:
     def doc_ids(self) -> np.ndarray:
         return np.ctypeslib.as_array(self._ptr.contents.doc_ids, shape=(self.num_tokens,)).copy()
 
+    def split_docs(self, docs) -> "BorrowedCorpus":
+        """The corpus restricted to the given docs (renumbered 0.. in the given
+        order) over the same vocabulary: word ids and V are kept, so a model
+        trained on the other docs applies to it (fold-in of held-out docs)."""
+        docs = np.asarray(docs, dtype=np.int64)
+        remap = np.full(self.num_docs, -1, dtype=np.int64)
+        remap[docs] = np.arange(len(docs))
+        ids = self.doc_ids
+        word_of = np.repeat(np.arange(self.num_words), np.diff(self.word_ptr))
+        keep = remap[ids] >= 0
+        new_ids = remap[ids[keep]]
+        new_words = word_of[keep]
+        order = np.lexsort((new_ids, new_words))  # word-major, ascending doc id within a word
+        new_ids = new_ids[order].astype(np.int32)
+        counts = np.bincount(new_words, minlength=self.num_words)
+        word_ptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        lens = np.diff(self.doc_ptr)[docs]
+        doc_ptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        return BorrowedCorpus(doc_ptr, word_ptr, new_ids)
+
     def doc_tokens(self) -> np.ndarray:
         """docRevIdx: word-major token ids grouped by doc (doc_chunk.cpp:225-255)."""
         out = np.empty(self.num_tokens, dtype=np.int32)

@@ -27,60 +27,12 @@
 #include <string>
 #include <vector>
 
+#include "context.h"
 #include "kernels.cuh"
 #include "philox.h"
 
 using namespace culda;
 
-struct culda_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    culda_params params{};
-    int32_t D = 0, V = 0, K = 0;
-    int64_t N = 0;
-    int group_lanes = 8;
-    int sample_blocks = kSampleBlocksDefault;
-    int tuned = 0;
-    bool tune_pending = false;  // time the variants before iteration kTuneIteration
-    float tune_ms = 0.f;
-    int item_tokens = 0;
-
-    int64_t *d_word_ptr = nullptr, *d_doc_ptr = nullptr;
-    // Tokens are stored word by word as in the input, but inside each word
-    // ordered by their doc's length; d_tok_index[i] is the input (word-major)
-    // index of stored token i, the key of its Philox stream and of copy-out.
-    int32_t *d_doc_ids = nullptr, *d_doc_tok = nullptr, *d_doc_order = nullptr, *d_tok_index = nullptr;
-    uint16_t *d_z[2] = {nullptr, nullptr};
-    uint16_t *d_zx = nullptr;  // topics in input order for copy-in / copy-out
-    float *d_u = nullptr;      // the tokens' uniforms of the current iteration
-    int cur = 0;
-    ThetaEntry *d_theta = nullptr;
-    int64_t theta_cap = 0;
-    int2 *d_rows = nullptr;
-    int32_t *d_nk = nullptr;
-    culda_item *d_items = nullptr, *d_hot_items = nullptr;
-    int32_t num_items = 0, num_hot_items = 0, num_hot = 0;
-    int32_t *d_seg_start = nullptr;  // first stored token of every segment
-    int32_t num_segs = 0;
-    int32_t *d_hot_phi = nullptr;
-    double *d_item_ll = nullptr;
-    int32_t *d_counter = nullptr;
-    uint32_t *d_iter = nullptr;
-    DevStats *d_stats = nullptr;
-    int32_t *d_error = nullptr;
-    DevStats *h_stats = nullptr;  // pinned
-
-    int sample_grid = 1, theta_grid = 1;
-    double doc_term = 0;  // sum_d L_d * log(L_d + K alpha)
-    std::vector<int64_t> h_doc_ptr;
-    std::vector<int32_t> h_max_ia;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // recorded inside the iteration graph around the sampling and rebuild kernels
-    cudaEvent_t ev_s0 = nullptr, ev_s1 = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
-    uint32_t next_iteration = 1;
-    std::string err;
-};
 
 namespace {
 
@@ -141,6 +93,7 @@ void tune_store(const std::string &key, const TuneResult &r) {
     f << key << ' ' << r.group_lanes << ' ' << r.sample_blocks << ' ' << r.ms << '\n';
 }
 
+}  // namespace
 
 int fail(culda_ctx *c, int code, const char *fmt, ...) {
     char buf[512];
@@ -153,18 +106,6 @@ int fail(culda_ctx *c, int code, const char *fmt, ...) {
     return code;
 }
 
-#define CK(call)                                                                                           \
-    do {                                                                                                   \
-        cudaError_t e_ = (call);                                                                           \
-        if (e_ != cudaSuccess)                                                                             \
-            return fail(ctx, e_ == cudaErrorMemoryAllocation ? CULDA_ERR_OOM : CULDA_ERR_CUDA, "%s: %s (%s:%d)", \
-                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                                \
-    } while (0)
-
-template <class T>
-cudaError_t dalloc(T **p, size_t n) {
-    return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
-}
 
 // Sampler parameters for topics d_z[cur] -> d_z[1-cur]; the Philox iteration
 // comes from the device counter when iteration_ptr is set (graph launches).
@@ -192,6 +133,8 @@ SampleParams sample_params(const culda_ctx *ctx, int cur, uint32_t iteration, co
     p.seg_start = ctx->d_seg_start;
     p.num_segs = ctx->num_segs;
     p.hot_phi = ctx->d_hot_phi;
+    p.frozen_phi = ctx->d_frozen_phi;
+    if (ctx->d_frozen_phi) p.nk = ctx->d_frozen_nk;
     p.item_counter = ctx->d_counter;
     p.item_ll = ctx->d_item_ll;
     p.seed = ctx->params.seed;
@@ -201,7 +144,11 @@ SampleParams sample_params(const culda_ctx *ctx, int cur, uint32_t iteration, co
     return p;
 }
 
+namespace {
+
 __global__ void copy_error_kernel(const int32_t *err, DevStats *st) { st->error = *err; }
+
+}  // namespace
 
 // Inside a stream capture a plain event record only orders the capture; the
 // external flag turns it into an event-record node of the graph so the event
@@ -214,10 +161,12 @@ cudaError_t record_event(cudaEvent_t ev, cudaStream_t s) {
                                                : cudaEventRecord(ev, s);
 }
 
+namespace {
+
 int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
     const int nxt = 1 - cur;
     CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
-    if (ctx->num_hot > 0) {
+    if (ctx->num_hot > 0 && !ctx->d_frozen_phi) {
         CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
         CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
                            s));
@@ -241,6 +190,8 @@ int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
     return CULDA_OK;
 }
 
+}  // namespace
+
 // Rebuild theta rows and n_k from the current topics (set-up and set_topics).
 int rebuild_counts(culda_ctx *ctx) {
     cudaStream_t s = ctx->stream;
@@ -255,6 +206,8 @@ int rebuild_counts(culda_ctx *ctx) {
     if (e) return fail(ctx, CULDA_ERR_DEVICE_STATE, "theta rebuild reported device error 0x%x", e);
     return CULDA_OK;
 }
+
+namespace {
 
 constexpr uint32_t kTuneIteration = 3;
 
@@ -279,7 +232,7 @@ int autotune_sampler(culda_ctx *ctx) {
     }
     cudaStream_t s = ctx->stream;
     const int cur = ctx->cur;
-    if (ctx->num_hot > 0) {
+    if (ctx->num_hot > 0 && !ctx->d_frozen_phi) {
         CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
         CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
                            s));
@@ -325,6 +278,8 @@ int autotune_sampler(culda_ctx *ctx) {
     return CULDA_OK;
 }
 
+}  // namespace
+
 int build_graphs(culda_ctx *ctx) {
     for (int c = 0; c < 2; ++c) {
         if (ctx->graph[c]) {
@@ -347,6 +302,8 @@ int build_graphs(culda_ctx *ctx) {
     }
     return CULDA_OK;
 }
+
+namespace {
 
 int pick_group_lanes(int requested, int k) {
     if (requested == 1 || requested == 2 || requested == 4 || requested == 8 || requested == 16 || requested == 32)
@@ -872,7 +829,7 @@ extern "C" int culda_iterate(culda_ctx *ctx, int n, culda_iter_stats *stats) {
 }
 
 // Device topics in stored order -> host array in input (word-major) order.
-static int topics_to_host(culda_ctx *ctx, const uint16_t *d_src, uint16_t *host) {
+int topics_to_host(culda_ctx *ctx, const uint16_t *d_src, uint16_t *host) {
     cudaStream_t s = ctx->stream;
     if (ctx->d_tok_index) {
         CK(launch_scatter<uint16_t>(ctx->N, ctx->d_tok_index, d_src, ctx->d_zx, s));
@@ -965,7 +922,7 @@ extern "C" int culda_sample_snapshot(culda_ctx *ctx, uint32_t iteration, uint16_
     cudaStream_t s = ctx->stream;
     const int cur = ctx->cur, nxt = 1 - cur;
     CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
-    if (ctx->num_hot > 0) {
+    if (ctx->num_hot > 0 && !ctx->d_frozen_phi) {
         CK(cudaMemsetAsync(ctx->d_hot_phi, 0, sizeof(int32_t) * (size_t)ctx->num_hot * ctx->K, s));
         CK(launch_hot_rows(ctx->K, ctx->d_hot_items, ctx->num_hot_items, ctx->d_z[cur], ctx->d_hot_phi, ctx->d_error,
                            s));
@@ -1049,6 +1006,7 @@ extern "C" void culda_destroy(culda_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_learned_state(ctx);
     for (int c = 0; c < 2; ++c)
         if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
     void *bufs[] = {ctx->d_word_ptr, ctx->d_doc_ptr, ctx->d_doc_ids,  ctx->d_doc_tok,  ctx->d_doc_order,

@@ -293,6 +293,12 @@ cudaError_t gemm(int M, int N, int K, const bf16 *A, const bf16 *B, int epi, con
 }  // namespace
 
 int encoder_k(const culda_encoder *e) { return e->K; }
+int encoder_num_words(const culda_encoder *e) { return e->V; }
+float *encoder_tensor(culda_encoder *e, int t) { return e->tensor(t); }
+int encoder_refresh(culda_encoder *e, cudaStream_t s) {
+    ECK(refresh_bf16(e, s));
+    return CULDA_OK;
+}
 int encoder_max_batch(const culda_encoder *e) { return e->Bmax; }
 int32_t *encoder_error_word(culda_encoder *e) { return e->d_error; }
 

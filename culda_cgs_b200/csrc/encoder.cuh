@@ -27,6 +27,12 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
 // Mean cross-entropy of the passes since the last call (synchronises s).
 int encoder_take_loss(culda_encoder *e, int batch_rows, double *loss, cudaStream_t s);
 
+// FP32 master copy of tensor t (CULDA_ENC_*) and the BF16 refresh after a
+// direct write to it.
+float *encoder_tensor(culda_encoder *e, int t);
+int encoder_refresh(culda_encoder *e, cudaStream_t s);
+int encoder_num_words(const culda_encoder *e);
+
 int encoder_k(const culda_encoder *e);
 int encoder_max_batch(const culda_encoder *e);
 int32_t *encoder_error_word(culda_encoder *e);

@@ -40,6 +40,8 @@ struct SampleParams {
     const int32_t *seg_start;    // [num_segs] first token of every segment
     int32_t num_segs;
     const int32_t *hot_phi;      // [num_hot * K]
+    const int32_t *frozen_phi;   // [V * K] word-topic counts held fixed (fold-in), or null; then nk
+                                 // holds the matching topic totals
     int32_t *item_counter;       // work queue head, zeroed before the launch
     double *item_ll;             // [num_items] sum of log(S+Q) per item
     uint64_t seed;

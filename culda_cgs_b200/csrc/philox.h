@@ -63,7 +63,8 @@ enum : uint32_t {
     kPurposeAccept = 3u,
     kPurposeWeights = 4u,   // encoder weight initialisation
     kPurposeShuffle = 5u,   // encoder training batch order
-    kPurposeWarm = 6u       // encoder warm start of new documents' topics
+    kPurposeWarm = 6u,      // encoder warm start of new documents' topics
+    kPurposeMH = 16u        // Metropolis-Hastings step j of an iteration uses kPurposeMH + j
 };
 
 // All four words of one Philox block.

@@ -313,7 +313,9 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_kernel(const Samp
 
         // phi row of the word
         const int *src;
-        if (item.hot < 0) {
+        if (p.frozen_phi) {
+            src = p.frozen_phi + (size_t)item.word * K;
+        } else if (item.hot < 0) {
             for (int j = tid; j < K; j += blockDim.x) hist[j] = 0;
             __syncthreads();
             for (int64_t t = ibeg + tid; t < iend; t += blockDim.x) {

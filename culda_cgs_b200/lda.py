@@ -59,13 +59,65 @@ class LDA:
     def _check(self, status: int) -> None:
         check(status, self._ctx)
 
+    @staticmethod
+    def _stats(st, n) -> list[dict]:
+        return [{name: getattr(s, name) for name, _ in _ffi.IterStats._fields_} for s in st[:n]]
+
     def iterate(self, n: int = 1) -> list[dict]:
         st = (_ffi.IterStats * max(n, 1))()
         self._check(lib().culda_iterate(self._ctx, int(n), st))
-        return [dict(iteration=s.iteration, status=s.status, seconds=s.seconds, loglik=s.loglik,
-                     tokens_per_sec=s.tokens_per_sec, row_entries=s.row_entries, theta_nnz=s.theta_nnz,
-                     token_nnz=s.token_nnz, sample_seconds=s.sample_seconds, rebuild_seconds=s.rebuild_seconds)
-                for s in st[:n]]
+        return self._stats(st, n)
+
+    # ---------------------------------------------------- learned proposal
+    def accumulate_theta(self) -> None:
+        """Adds the current doc-topic counts to the encoder's training targets."""
+        self._check(lib().culda_accumulate_theta(self._ctx))
+
+    def init_encoder(self, encoder, seed: int = 1) -> None:
+        """Word embeddings from the current topics' word profiles (a random projection)."""
+        self._check(lib().culda_encoder_init_from_phi(self._ctx, encoder.handle, int(seed)))
+
+    def train_encoder(self, encoder, epochs: int, seed: int = 1) -> float:
+        loss = C.c_double()
+        self._check(lib().culda_train_encoder(self._ctx, encoder.handle, int(epochs), int(seed), C.byref(loss)))
+        return loss.value
+
+    def set_proposal(self, encoder, mix: float = 0.05) -> None:
+        """The encoder's per-doc distributions (mixed with mix / K) become the
+        independent MH proposal; None drops it."""
+        self._check(lib().culda_set_proposal(self._ctx, encoder.handle if encoder is not None else None,
+                                             float(mix)))
+
+    def proposal(self) -> np.ndarray:
+        cdf = np.empty((self.num_docs, self.k), dtype=np.float32)
+        self._check(lib().culda_get_proposal(self._ctx, cdf.ctypes.data_as(C.c_void_p)))
+        return cdf
+
+    def iterate_mh(self, n: int = 1, steps: int = 2) -> list[dict]:
+        st = (_ffi.IterStats * max(n, 1))()
+        self._check(lib().culda_iterate_mh(self._ctx, int(n), int(steps), st))
+        return self._stats(st, n)
+
+    def mh_snapshot(self, iteration: int, steps: int = 2) -> np.ndarray:
+        z = np.empty(self.num_tokens, dtype=np.uint16)
+        self._check(lib().culda_mh_snapshot(self._ctx, int(iteration), int(steps), z.ctypes.data_as(C.c_void_p)))
+        return z
+
+    # -------------------------------------------------------------- fold-in
+    def set_frozen_phi(self, phi, nk) -> None:
+        """Sample this corpus against fixed word-topic counts (None: own counts)."""
+        if phi is None:
+            self._check(lib().culda_set_frozen_phi(self._ctx, None, None))
+            return
+        phi = np.ascontiguousarray(phi, dtype=np.int32)
+        nk = np.ascontiguousarray(nk, dtype=np.int32)
+        assert phi.shape == (self.num_words, self.k) and nk.shape == (self.k,)
+        self._check(lib().culda_set_frozen_phi(self._ctx, phi.ctypes.data_as(C.c_void_p),
+                                               nk.ctypes.data_as(C.c_void_p)))
+
+    def warm_start(self) -> None:
+        """Topics drawn from the proposal (set_proposal) times phihat."""
+        self._check(lib().culda_warm_start(self._ctx))
 
     def topics(self) -> np.ndarray:
         z = np.empty(self.num_tokens, dtype=np.uint16)

@@ -177,6 +177,7 @@ typedef struct culda_iter_stats {
     int64_t token_nnz;      /* sum over tokens of the non-zeros in their doc's rebuilt row */
     double sample_seconds;  /* device time of the sampler kernel */
     double rebuild_seconds; /* device time of the theta / n_k rebuild */
+    double accept_rate;     /* Metropolis-Hastings iterations: accepted moves / proposals (else 0) */
 } culda_iter_stats;
 
 typedef struct culda_ctx culda_ctx;
@@ -456,6 +457,70 @@ int culda_encoder_backward(culda_encoder *e, int32_t batch, const int32_t *d_doc
 /* culda_encoder_backward followed by one Adam step on every weight. */
 int culda_encoder_train_step(culda_encoder *e, int32_t batch, const int32_t *d_docs, const int64_t *d_doc_ptr,
                              const int32_t *d_words, const float *d_target, double *loss, void *stream);
+
+/* ----------------------------------- learned proposal (no reference counterpart)
+ * Training data, the encoder proposal and Metropolis-Hastings iterations on a
+ * context.  The target of every MH step is the plain sampler's conditional on
+ * the frozen snapshot of the iteration, p(k) ~ (n_dk + alpha) phihat_wk, so
+ * the chain's target is unchanged; plain CGS (culda_iterate) can be mixed in
+ * at any point. */
+
+/* Adds the current state's doc-topic counts to the context's training
+ * accumulator (D x K FP32, allocated on the first call). */
+int culda_accumulate_theta(culda_ctx *ctx);
+
+/* Trains enc on (document, accumulated topic distribution) pairs with target
+ * (acc_dk / n + alpha) / (L_d + K alpha), n the accumulated states: `epochs`
+ * passes over the docs in a Philox-shuffled order (key `seed`), batches of the
+ * encoder's max_batch.  *loss: mean cross-entropy of the last epoch.  The
+ * encoder's num_words and k must match the context. */
+int culda_train_encoder(culda_ctx *ctx, culda_encoder *enc, int32_t epochs, uint64_t seed, double *loss);
+
+/* Sets enc's word embeddings from the context's current topics: row w is the
+ * word's topic profile (n_wk + beta) / (n_w + K beta) projected to 256
+ * dimensions by a fixed random matrix (Philox key `seed`, entries of unit
+ * variance; a tensor-core GEMM) and scaled to root-mean-square 0.3, so a
+ * document's bag mean starts out as a projection of its words' topic
+ * profiles.  The other weights are left as they are. */
+int culda_encoder_init_from_phi(culda_ctx *ctx, culda_encoder *enc, uint64_t seed);
+
+/* Runs enc over every doc and keeps, per doc, the proposal
+ * (1 - mix) q_d + mix / K as an inclusive prefix table (FP32 D x K).  enc NULL
+ * drops the proposal.  mix in [0, 1). */
+int culda_set_proposal(culda_ctx *ctx, culda_encoder *enc, float mix);
+
+/* The prefix table of culda_set_proposal, D x K FP32 in doc order (host). */
+int culda_get_proposal(culda_ctx *ctx, float *cdf);
+
+/* n Metropolis-Hastings iterations: per token `steps` steps (1..64) from its
+ * current topic, alternating the doc proposal (n_dk + alpha, acceptance
+ * phihat_wk' / phihat_wk) and, when a proposal is set, the encoder proposal
+ * (independent, acceptance p(k') q_d(k) / (p(k) q_d(k'))); without one every
+ * step uses the doc proposal.  Uniforms: Philox (seed, token, iteration,
+ * 16 + step).  The counts are then rebuilt as after a plain iteration.  stats:
+ * loglik is NaN (evaluate with culda_sample_snapshot), sample_seconds is the
+ * MH kernel, accept_rate is set. */
+int culda_iterate_mh(culda_ctx *ctx, int32_t n, int32_t steps, culda_iter_stats *stats);
+
+/* One MH pass of `steps` steps from the current snapshot with Philox
+ * iteration `iteration`, leaving the state unchanged; topics to host in input
+ * order (topics_out may be NULL). */
+int culda_mh_snapshot(culda_ctx *ctx, uint32_t iteration, int32_t steps, uint16_t *topics_out);
+
+/* ------------------------------------------------ fold-in (no reference counterpart)
+ * New documents sampled against a trained model: the context's samplers (plain
+ * and MH) use the given word-topic counts phi [V x K] and topic totals nk [K]
+ * (host arrays over the same vocabulary, e.g. culda_get_phi of the trained
+ * context) instead of its own corpus's counts; theta stays the new documents'.
+ * The per-iteration log-likelihood is then the held-out per-token value under
+ * the frozen model.  phi NULL returns to the context's own counts.  Rows must
+ * sum to nk. */
+int culda_set_frozen_phi(culda_ctx *ctx, const int32_t *phi, const int32_t *nk);
+
+/* Warm start from the proposal set by culda_set_proposal: every token's topic
+ * is drawn from q_d(k) * phihat_wk (Philox: seed, token, 0, 6), then the
+ * counts are rebuilt. */
+int culda_warm_start(culda_ctx *ctx);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -291,11 +291,28 @@ static inline void neumaier_add(double &sum, double &comp, double x) {
     sum = t;
 }
 
+/* phi_fixed [V x K] (with nk its totals) replaces the counts of z: fold-in
+ * against a frozen model (no reference counterpart). */
+void oracle_sample_fixed_fp64(int32_t num_docs, int32_t num_words, int32_t k, float alpha_f, float beta_f,
+                              const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr,
+                              const uint16_t *z, const int32_t *nk, const int16_t *theta_a, const int16_t *theta_ja,
+                              const int32_t *max_ia, const int32_t *cur_ia, uint64_t seed, uint32_t iteration,
+                              const int32_t *phi_fixed, uint16_t *z_out, double *margin, double *loglik_terms);
+
 void oracle_sample_fp64(int32_t num_docs, int32_t num_words, int32_t k, float alpha_f, float beta_f,
                         const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr, const uint16_t *z,
                         const int32_t *nk, const int16_t *theta_a, const int16_t *theta_ja, const int32_t *max_ia,
                         const int32_t *cur_ia, uint64_t seed, uint32_t iteration, uint16_t *z_out, double *margin,
                         double *loglik_terms) {
+    oracle_sample_fixed_fp64(num_docs, num_words, k, alpha_f, beta_f, word_ptr, doc_ids, doc_ptr, z, nk, theta_a,
+                             theta_ja, max_ia, cur_ia, seed, iteration, nullptr, z_out, margin, loglik_terms);
+}
+
+void oracle_sample_fixed_fp64(int32_t num_docs, int32_t num_words, int32_t k, float alpha_f, float beta_f,
+                              const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr,
+                              const uint16_t *z, const int32_t *nk, const int16_t *theta_a, const int16_t *theta_ja,
+                              const int32_t *max_ia, const int32_t *cur_ia, uint64_t seed, uint32_t iteration,
+                              const int32_t *phi_fixed, uint16_t *z_out, double *margin, double *loglik_terms) {
     const double alpha = alpha_f, beta = beta_f;
     const double vbeta = (double)num_words * beta;
     std::vector<double> inv((size_t)k), ph((size_t)k);
@@ -304,7 +321,10 @@ void oracle_sample_fp64(int32_t num_docs, int32_t num_words, int32_t k, float al
     double s_log = 0, c_log = 0, s_doc = 0, c_doc = 0;
     for (int32_t w = 0; w < num_words; ++w) {
         std::fill(hist.begin(), hist.end(), 0);
-        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) hist[z[t]]++;
+        if (phi_fixed)
+            std::copy(phi_fixed + (size_t)w * k, phi_fixed + (size_t)(w + 1) * k, hist.begin());
+        else
+            for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) hist[z[t]]++;
         double q = 0;
         for (int32_t j = 0; j < k; ++j) {
             ph[j] = ((double)hist[j] + beta) / ((double)nk[j] + vbeta);
@@ -369,6 +389,126 @@ void oracle_sample_fp64(int32_t num_docs, int32_t num_words, int32_t k, float al
     if (loglik_terms) {
         loglik_terms[0] = s_log + c_log;
         loglik_terms[1] = s_doc + c_doc;
+    }
+}
+
+/* ------------------------------------ Metropolis-Hastings (no reference counterpart) */
+/*
+ * One MH pass from the snapshot z (input order), restating
+ * culda_cgs_b200/csrc/learned.cu in FP64 on the same Philox words
+ * (counter {t, iteration, 16 + step}): per token `steps` steps, even steps (all
+ * steps when cdf is NULL) the doc proposal (n_dk + alpha) with acceptance
+ * phihat_wk' / phihat_ws, odd steps the independent proposal given by the
+ * prefix table cdf [D x K] with acceptance p(k') q(s) / (p(s) q(k')),
+ * p(k) = (n_dk + alpha) phihat_wk.  margin[t]: the smallest relative distance
+ * of any decision on the token's path (bucket choice, table search,
+ * acceptance) to its boundary.
+ */
+static inline void philox_words(uint64_t seed, uint64_t t, uint32_t iter, uint32_t purpose, uint32_t out[4]) {
+    uint32_t ctr[4] = {(uint32_t)t, (uint32_t)(t >> 32), iter, purpose};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    oracle_philox4x32_10(ctr, key, out);
+}
+
+static inline uint32_t bounded(uint32_t x, uint32_t n) { return (uint32_t)(((uint64_t)x * (uint64_t)n) >> 32); }
+
+void oracle_mh_fp64(int32_t num_docs, int32_t num_words, int32_t k, float alpha_f, float beta_f,
+                    const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr, const int32_t *doc_tok,
+                    const uint16_t *z, const int32_t *nk, const float *cdf, uint64_t seed, uint32_t iteration,
+                    int32_t steps, uint16_t *z_out, double *margin) {
+    const double alpha = alpha_f, beta = beta_f, vbeta = (double)num_words * beta, ka = (double)k * alpha;
+    std::vector<int32_t> ndk((size_t)num_docs * k, 0);
+    for (int32_t d = 0; d < num_docs; ++d)
+        for (int64_t i = doc_ptr[d]; i < doc_ptr[d + 1]; ++i) ndk[(size_t)d * k + z[doc_tok[i]]]++;
+    std::vector<double> ph((size_t)k);
+    std::vector<int32_t> hist((size_t)k);
+    for (int32_t w = 0; w < num_words; ++w) {
+        std::fill(hist.begin(), hist.end(), 0);
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) hist[z[t]]++;
+        for (int32_t j = 0; j < k; ++j) ph[j] = ((double)hist[j] + beta) / ((double)nk[j] + vbeta);
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) {
+            const int32_t d = doc_ids[t];
+            const int64_t d0 = doc_ptr[d];
+            const double L = (double)(doc_ptr[d + 1] - d0);
+            int32_t s = z[t];
+            double m = INFINITY;
+            for (int32_t step = 0; step < steps; ++step) {
+                uint32_t x[4];
+                philox_words(seed, (uint64_t)t, iteration, 16u + (uint32_t)step, x);
+                int32_t kp;
+                double ratio;
+                if (!(cdf && (step & 1))) {
+                    const double a = oracle_uniform(x[0]) * (L + ka);
+                    m = std::min(m, std::fabs(a - L) / (L + ka));
+                    if (a < L)
+                        kp = z[doc_tok[d0 + bounded(x[1], (uint32_t)L)]];
+                    else
+                        kp = (int32_t)bounded(x[1], (uint32_t)k);
+                    ratio = ph[kp] / ph[s];
+                } else {
+                    const float *row = cdf + (size_t)d * k;
+                    const double total = row[k - 1];
+                    const double T = oracle_uniform(x[1]) * total;
+                    kp = k - 1;
+                    for (int32_t j = 0; j < k; ++j)
+                        if ((double)row[j] > T) {
+                            kp = j;
+                            break;
+                        }
+                    const double lo = kp > 0 ? (double)row[kp - 1] : 0.0;
+                    m = std::min(m, std::min((double)row[kp] - T, T - lo) / total);
+                    const double qk = (double)row[kp] - lo;
+                    const double qs = (double)row[s] - (s > 0 ? (double)row[s - 1] : 0.0);
+                    const double pk = ((double)ndk[(size_t)d * k + kp] + alpha) * ph[kp];
+                    const double ps = ((double)ndk[(size_t)d * k + s] + alpha) * ph[s];
+                    ratio = (pk * qs) / (ps * qk);
+                }
+                if (kp != s) {
+                    const double u = oracle_uniform(x[2]);
+                    if (ratio > 0) m = std::min(m, std::fabs(u - ratio) / ratio);
+                    if (u < ratio) s = kp;
+                }
+            }
+            z_out[t] = (uint16_t)s;
+            if (margin) margin[t] = m;
+        }
+    }
+}
+
+/* Warm start (no reference counterpart; culda_cgs_b200/csrc/learned.cu): token
+ * t of word w in doc d draws its topic from q_d(k) * phihat_wk, q_d(k) the
+ * differences of the prefix table cdf [D x K], phihat from phi [V x K] and nk,
+ * by inverse CDF in ascending topic with u = Philox(seed, {t, 0, 6}). */
+void oracle_warm_start(int32_t num_docs, int32_t num_words, int32_t k, float beta_f, const int64_t *word_ptr,
+                       const int32_t *doc_ids, const int32_t *phi, const int32_t *nk, const float *cdf, uint64_t seed,
+                       uint16_t *z_out, double *margin) {
+    (void)num_docs;
+    const double beta = beta_f, vbeta = (double)num_words * beta;
+    std::vector<double> ph((size_t)k), p((size_t)k);
+    for (int32_t w = 0; w < num_words; ++w) {
+        for (int32_t j = 0; j < k; ++j) ph[j] = ((double)phi[(size_t)w * k + j] + beta) / ((double)nk[j] + vbeta);
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) {
+            const float *row = cdf + (size_t)doc_ids[t] * k;
+            double total = 0;
+            for (int32_t j = 0; j < k; ++j) {
+                p[j] = ((double)row[j] - (j > 0 ? (double)row[j - 1] : 0.0)) * ph[j];
+                total += p[j];
+            }
+            const double T = oracle_uniform(philox_word0(seed, (uint64_t)t, 0u, 6u)) * total;
+            double cum = 0, lo = 0, hi = total;
+            int32_t pick = k - 1;
+            for (int32_t j = 0; j < k; ++j) {
+                if (cum + p[j] > T) {
+                    pick = j;
+                    lo = cum;
+                    hi = cum + p[j];
+                    break;
+                }
+                cum += p[j];
+            }
+            z_out[t] = (uint16_t)pick;
+            if (margin) margin[t] = std::min(T - lo, hi - T) / total;
+        }
     }
 }
 

@@ -188,18 +188,49 @@ class Snapshot:
         return cls(d, v, k, float(np.float32(alpha)), float(np.float32(beta)), word_ptr, doc_ids, doc_ptr, doc_tok, z,
                    phi, nk, a, ja, max_ia, cur)
 
-    def sample(self, seed: int, iteration: int):
-        """(z_new, margin, loglik): one FP64 draw per token on this snapshot."""
+    def sample(self, seed: int, iteration: int, phi=None, nk=None):
+        """(z_new, margin, loglik): one FP64 draw per token on this snapshot;
+        with phi / nk given, against those fixed word-topic counts (fold-in)."""
         n = len(self.z)
         z_out = np.empty(n, dtype=np.uint16)
         margin = np.empty(n, dtype=np.float64)
         terms = np.zeros(2, dtype=np.float64)
-        lib().oracle_sample_fp64(C.c_int32(self.num_docs), C.c_int32(self.num_words), C.c_int32(self.k),
-                                 C.c_float(self.alpha), C.c_float(self.beta), _p(self.word_ptr), _p(self.doc_ids),
-                                 _p(self.doc_ptr), _p(self.z), _p(self.nk), _p(self.theta_a), _p(self.theta_ja),
-                                 _p(self.max_ia), _p(self.cur_ia), C.c_uint64(seed), C.c_uint32(iteration), _p(z_out),
-                                 _p(margin), _p(terms))
+        fixed = _c(phi, np.int32) if phi is not None else None
+        nk_used = _c(nk, np.int32) if phi is not None else self.nk
+        lib().oracle_sample_fixed_fp64(C.c_int32(self.num_docs), C.c_int32(self.num_words), C.c_int32(self.k),
+                                       C.c_float(self.alpha), C.c_float(self.beta), _p(self.word_ptr),
+                                       _p(self.doc_ids), _p(self.doc_ptr), _p(self.z), _p(nk_used), _p(self.theta_a),
+                                       _p(self.theta_ja), _p(self.max_ia), _p(self.cur_ia), C.c_uint64(seed),
+                                       C.c_uint32(iteration), _p(fixed) if fixed is not None else None, _p(z_out),
+                                       _p(margin), _p(terms))
         return z_out, margin, (terms[0] - terms[1]) / n
+
+    def mh(self, seed: int, iteration: int, steps: int, cdf=None):
+        """(z_new, margin): one Metropolis-Hastings pass from this snapshot
+        (oracle_mh_fp64); cdf is the [D x K] float32 proposal prefix table or None."""
+        n = len(self.z)
+        z_out = np.empty(n, dtype=np.uint16)
+        margin = np.empty(n, dtype=np.float64)
+        c = None if cdf is None else _c(cdf, np.float32)
+        lib().oracle_mh_fp64(C.c_int32(self.num_docs), C.c_int32(self.num_words), C.c_int32(self.k),
+                             C.c_float(self.alpha), C.c_float(self.beta), _p(self.word_ptr), _p(self.doc_ids),
+                             _p(self.doc_ptr), _p(self.doc_tok), _p(self.z), _p(self.nk),
+                             _p(c) if c is not None else None, C.c_uint64(seed), C.c_uint32(iteration),
+                             C.c_int32(steps), _p(z_out), _p(margin))
+        return z_out, margin
+
+    def warm_start(self, seed: int, cdf, phi=None, nk=None):
+        """(z, margin): topics drawn from q_d(k) * phihat_wk (oracle_warm_start)."""
+        n = len(self.z)
+        z_out = np.empty(n, dtype=np.uint16)
+        margin = np.empty(n, dtype=np.float64)
+        phi = _c(self.phi if phi is None else phi, np.int32)
+        nk = _c(self.nk if nk is None else nk, np.int32)
+        c = _c(cdf, np.float32)
+        lib().oracle_warm_start(C.c_int32(self.num_docs), C.c_int32(self.num_words), C.c_int32(self.k),
+                                C.c_float(self.beta), _p(self.word_ptr), _p(self.doc_ids), _p(phi), _p(nk), _p(c),
+                                C.c_uint64(seed), _p(z_out), _p(margin))
+        return z_out, margin
 
     def loglik_joint(self) -> float:
         f = lib().oracle_loglik_joint

@@ -191,6 +191,110 @@ def ncu_traffic(workload: str):
         return None
 
 
+# ----------------------------------------------- learned form and fold-in
+def measure_learned(args, wl, corpus, device) -> dict:
+    """Wall-clock to the plain chain's iteration-100 log-likelihood, plain CGS
+    against the learned form: plain iterations 1-40 with states 21-40
+    accumulated, the encoder initialised from the word profiles and trained on
+    them, then Metropolis-Hastings iterations mixing the doc and encoder
+    proposals 1:1 (2 steps per token).  Every state's log-likelihood is the
+    per-token value of culda_sample_snapshot (evaluation passes are not
+    timed); iterations are timed with CUDA events, the host-driven steps
+    (accumulation, training, proposal tables) by the wall clock."""
+    import culda_cgs_b200 as cb
+
+    target_it, first, window, epochs, max_mh = 100, 20, 20, args.learned_epochs, 60
+    with cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device) as m:
+        st = m.iterate(target_it)
+        t_plain = sum(x["seconds"] for x in st)
+        target = m.sample_snapshot(1 << 30)[1]
+        plain_curve = [(i + 1, round(sum(x["seconds"] for x in st[:i + 1]), 4)) for i in (39, 59, 79, 99)]
+    out = {"target": "log-likelihood per token of the plain chain's state after iteration 100",
+           "target_loglik": round(target, 6), "plain_seconds": round(t_plain, 4), "plain_seconds_at": plain_curve}
+    with cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device) as m, \
+            cb.Encoder(corpus.num_words, wl.k, args.learned_batch, seed=1, device=device) as enc:
+        t = sum(x["seconds"] for x in m.iterate(first))
+        for _ in range(window):
+            t += m.iterate(1)[0]["seconds"]
+            t0 = time.perf_counter()
+            m.accumulate_theta()
+            t += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        m.init_encoder(enc, seed=3)
+        losses = [m.train_encoder(enc, 1, seed=e) for e in range(epochs)]
+        m.set_proposal(enc, mix=0.05)
+        t_train = time.perf_counter() - t0
+        t += t_train
+        curve, reached, accept, mh_sec = [], None, [], []
+        it = first + window
+        while it < first + window + max_mh:
+            st = m.iterate_mh(5, steps=2)
+            it += 5
+            t += sum(x["seconds"] for x in st)
+            mh_sec += [x["seconds"] for x in st]
+            accept += [x["accept_rate"] for x in st]
+            ll = m.sample_snapshot(1 << 29)[1]
+            curve.append((it, round(t, 4), round(ll, 6)))
+            if ll >= target:
+                reached = t
+                break
+    out.update({
+        "schedule": f"plain 1-{first + window} (states {first + 1}-{first + window} accumulated), encoder "
+                    f"initialised from word profiles and trained {epochs} epochs (batch {args.learned_batch}), then "
+                    f"MH doc:encoder 1:1, 2 steps per token, up to {max_mh} iterations",
+        "learned_seconds_to_target": round(reached, 4) if reached else None,
+        "reached": reached is not None,
+        "ratio_learned_to_plain": round(reached / t_plain, 4) if reached else None,
+        "encoder_train_seconds": round(t_train, 4), "encoder_loss": [round(losses[0], 4), round(losses[-1], 4)],
+        "mh_ms_per_iteration": round(1e3 * statistics.mean(mh_sec), 4) if mh_sec else None,
+        "mh_accept_rate": round(statistics.mean(accept), 4) if accept else None,
+        "learned_curve": curve})
+    return out
+
+
+def measure_foldin(args, device) -> dict:
+    """Fold-in of 100k new documents (the SMALL generator, same vocabulary)
+    against the frozen counts of a model trained 50 iterations on 10k docs:
+    held-out log-likelihood per token per sweep from random initial topics and
+    from the encoder's warm start, and held-out docs per second per sweep."""
+    import numpy as np
+
+    import culda_cgs_b200 as cb
+    from culda_cgs_b200.configs import FOLDIN, FOLDIN_TRAIN_DOCS
+
+    wl = FOLDIN.with_seed(args.seed)
+    c = cb.Corpus.generate(wl.gen)
+    train = c.split_docs(np.arange(FOLDIN_TRAIN_DOCS))
+    held = c.split_docs(np.arange(FOLDIN_TRAIN_DOCS, c.num_docs))
+    sweeps = (1, 2, 5, 10, 20, 50)
+    out = {"workload": wl.name, "train_docs": train.num_docs, "train_tokens": train.num_tokens,
+           "held_docs": held.num_docs, "held_tokens": held.num_tokens}
+    with cb.LDA(train, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device) as m, \
+            cb.Encoder(c.num_words, wl.k, 512, seed=1, device=device) as enc:
+        m.iterate(30)
+        for _ in range(20):
+            m.iterate(1)
+            m.accumulate_theta()
+        phi, nk = m.phi()
+        t0 = time.perf_counter()
+        m.init_encoder(enc, seed=3)
+        m.train_encoder(enc, 20, seed=1)
+        out["encoder_train_seconds"] = round(time.perf_counter() - t0, 4)
+        for mode in ("random", "encoder"):
+            with cb.LDA(held, wl.k, wl.alpha, wl.beta, seed=args.seed + 1, device=device) as f:
+                f.set_frozen_phi(phi, nk)
+                if mode == "encoder":
+                    t0 = time.perf_counter()
+                    f.set_proposal(enc, mix=0.05)
+                    f.warm_start()
+                    out["warm_start_seconds"] = round(time.perf_counter() - t0, 4)
+                st = f.iterate(max(sweeps))
+                out[mode] = {f"sweep_{s}": round(st[s - 1]["loglik"], 6) for s in sweeps}
+                out[mode + "_docs_per_sec"] = round(held.num_docs / statistics.mean(x["seconds"] for x in st), 1)
+    out["loglik"] = "held-out per-token log-likelihood of the state before each sweep (FP64 sum of FP32 terms)"
+    return out
+
+
 # ------------------------------------------------------------------- ours
 def run_ours(args, world, rank, local, pg):
     import ctypes as C
@@ -308,6 +412,18 @@ def run_ours(args, world, rank, local, pg):
                          f"(set-up {setup:.1f}s untimed); oracle/cgs_cpu.cpp, same sampling rule, FP32, OpenMP"}
         h.close()
 
+    # ---- learned form vs plain, and fold-in (rank 0, one GPU only)
+    learned = foldin = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        try:
+            learned = measure_learned(args, wl, corpus, local)
+        except Exception as e:  # reported, never hides the main line
+            learned = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            foldin = measure_foldin(args, local)
+        except Exception as e:
+            foldin = {"error": f"{type(e).__name__}: {e}"}
+
     launches = info["kernels_per_iteration"] * args.steps
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -321,6 +437,7 @@ def run_ours(args, world, rank, local, pg):
                    "l2": f"inputs larger than L2 (resident set {info['device_bytes'] / 1e9:.2f} GB > 126 MB)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        "learned": learned, "foldin": foldin,
         "loglik": [round(s["loglik"], 8) for s in stats],
     }
     return line
@@ -402,6 +519,9 @@ def main():
     ap.add_argument("--cpu-iterations", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work at most")
     ap.add_argument("--ref-timeout", type=float, default=1200.0)
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-form and fold-in measurements")
+    ap.add_argument("--learned-epochs", type=int, default=8)
+    ap.add_argument("--learned-batch", type=int, default=1024)
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         ap.error("--steps >= 1 and --warmup >= 0")

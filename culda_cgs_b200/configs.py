@@ -49,6 +49,14 @@ UNEVEN = Workload("batched-uneven V=1M D=2M N~100M",
                   GenConfig(num_words=1_000_000, num_topics=1000, num_docs=2_000_000, len_law=CULDA_LEN_PARETO,
                             len_a=1.5, len_b=20.0, len_min=20, len_max=50_000, zipf_s=1.1), iterations=50)
 
+# Fold-in: the SMALL generator with 110k docs; the first 10k are the training
+# corpus (the SMALL shape), the other 100k are new documents over the same
+# vocabulary, sampled against the trained model's frozen counts.
+FOLDIN = Workload("foldin V=20k D=10k+100k K=1024",
+                  GenConfig(num_words=20_000, num_topics=100, num_docs=110_000, len_law=CULDA_LEN_POISSON,
+                            len_a=100.0, len_min=10, len_max=1000), iterations=50)
+FOLDIN_TRAIN_DOCS = 10_000
+
 # small corpora for tests
 TINY = Workload("tiny V=500 D=200 K=64",
                 GenConfig(num_words=500, num_topics=8, num_docs=200, len_law=CULDA_LEN_POISSON, len_a=40.0,
@@ -58,4 +66,4 @@ MINI = Workload("mini V=3k D=2k K=1024",
                 GenConfig(num_words=3_000, num_topics=40, num_docs=2_000, len_law=CULDA_LEN_LOGNORMAL, len_a=4.0,
                           len_b=0.8, len_min=1, len_max=1500), k=1024, iterations=5)
 
-WORKLOADS = {w.name.split()[0]: w for w in (SMALL, SCALE, MEDIUM, UNEVEN, TINY, MINI)}
+WORKLOADS = {w.name.split()[0]: w for w in (SMALL, SCALE, MEDIUM, UNEVEN, FOLDIN, TINY, MINI)}

@@ -154,6 +154,13 @@ def allreduce_max(pg, x: float) -> float:
     return float(t.item())
 
 
+def whole_job_rate(world: int, tokens_per_rank: int, steps: int, max_seconds: float) -> float:
+    """Tokens per second of the whole job: every rank samples its own replica
+    of tokens_per_rank tokens for `steps` iterations; the slowest rank's device
+    time bounds the job (weak scaling)."""
+    return world * tokens_per_rank * steps / max_seconds
+
+
 def barrier(pg):
     if pg is not None:
         pg.barrier()
@@ -330,7 +337,7 @@ def run_ours(args, world, rank, local, pg):
     clk = clocks.stop()
     dev_seconds = sum(s["seconds"] for s in stats)
     max_seconds = allreduce_max(pg, dev_seconds)
-    value = world * N * args.steps / max_seconds
+    value = whole_job_rate(world, N, args.steps, max_seconds)
     for s in stats:
         log(f"[rank {rank}] iteration {s['iteration']:4d}: {s['seconds'] * 1e3:8.3f} ms "
             f"(sample {s['sample_seconds'] * 1e3:.3f} ms, rebuild {s['rebuild_seconds'] * 1e3:.3f} ms) "

@@ -198,6 +198,18 @@ def ncu_traffic(workload: str):
         return None
 
 
+def workload(args, seed: int):
+    """The named workload with the run's seed; --k replaces K (and alpha = 50/K)."""
+    from dataclasses import replace
+
+    from culda_cgs_b200.configs import WORKLOADS
+
+    wl = WORKLOADS[args.workload].with_seed(seed)
+    if args.k:
+        wl = replace(wl, k=args.k, alpha=50.0 / args.k, name=f"{wl.name.split(' K=')[0]} K={args.k}")
+    return wl
+
+
 # ----------------------------------------------- learned form and fold-in
 def measure_learned(args, wl, corpus, device) -> dict:
     """Wall-clock to the plain chain's iteration-100 log-likelihood, plain CGS
@@ -311,7 +323,7 @@ def run_ours(args, world, rank, local, pg):
     import culda_cgs_b200 as cb
     from culda_cgs_b200.configs import WORKLOADS
 
-    wl = WORKLOADS[args.workload].with_seed(args.seed + rank)
+    wl = workload(args, args.seed + rank)
     t0 = time.perf_counter()
     corpus = cb.Corpus.generate(wl.gen)
     log(f"[rank {rank}] corpus {wl.name}: D={corpus.num_docs} V={corpus.num_words} N={corpus.num_tokens} "
@@ -331,6 +343,7 @@ def run_ours(args, world, rank, local, pg):
     cuda_sync()
     clocks.mark_start()
     stats = m.iterate(args.steps)
+    info = m.info()  # the variant in use (the autotuner may have changed it during warm-up)
     cuda_sync()
     barrier(pg)
     clocks.mark_end()
@@ -463,7 +476,7 @@ def run_reference(args, world, rank):
     import culda_cgs_b200 as cb
     from culda_cgs_b200.configs import WORKLOADS
 
-    wl = WORKLOADS[args.workload].with_seed(args.seed)
+    wl = workload(args, args.seed)
     if wl.k != 1024:
         return {"impl": "reference", "unavailable": "the reference kernel supports only K=1024"}
     corpus = cb.Corpus.generate(wl.gen)
@@ -516,6 +529,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="plain-cgs-scale")
+    ap.add_argument("--k", type=int, default=0, help="topics (default: the workload's); alpha = 50/K")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--group-lanes", type=int, default=0)
     ap.add_argument("--item-tokens", type=int, default=0)

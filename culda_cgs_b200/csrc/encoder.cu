@@ -126,25 +126,41 @@ __global__ void embbag_bwd_kernel(int batch, const int32_t *__restrict__ docs, c
         float4 g0 = src[0], g1 = src[1];
         g0 = make_float4(g0.x * inv, g0.y * inv, g0.z * inv, g0.w * inv);
         g1 = make_float4(g1.x * inv, g1.y * inv, g1.z * inv, g1.w * inv);
+        // runs of one word (a document's words arrive sorted when the CSR is
+        // the doc-ordered token list) are added with one atomic per column
+        int run_w = -1;
+        float mult = 0.f;
+        auto flush = [&]() {
+            if (run_w < 0) return;
+            float4 *dst = reinterpret_cast<float4 *>(gE + (size_t)run_w * kE) + 2 * lane;
+            atomicAdd(dst, make_float4(g0.x * mult, g0.y * mult, g0.z * mult, g0.w * mult));
+            atomicAdd(dst + 1, make_float4(g1.x * mult, g1.y * mult, g1.z * mult, g1.w * mult));
+        };
         for (int64_t tb = t0; tb < t1; tb += 32) {
             const int wl = tb + lane < t1 ? words[tb + lane] : 0;
             const int n = (int)min((int64_t)32, t1 - tb);
             for (int j = 0; j < n; ++j) {
                 const int w = __shfl_sync(0xffffffffu, wl, j);
                 if ((unsigned)w >= (unsigned)V) continue;  // reported by the forward pass
-                float4 *dst = reinterpret_cast<float4 *>(gE + (size_t)w * kE) + 2 * lane;
-                atomicAdd(dst, g0);
-                atomicAdd(dst + 1, g1);
+                if (w == run_w) {
+                    mult += 1.f;
+                } else {
+                    flush();
+                    run_w = w;
+                    mult = 1.f;
+                }
             }
         }
+        flush();
     }
 }
 
 // Softmax of each row of Z [rows x K] and, against the target, dZ = (q - t) /
 // batch (BF16), the column sums of dZ (db3) and the summed cross-entropy.
 // 256 threads = 8 warps per block, kXentRows rows per block; lane l holds
-// columns l, l+32, ... of its row.
-constexpr int kXentRows = 32;
+// columns l, l+32, ... of its row; the block's column sums go to db3 with one
+// atomic per column.
+constexpr int kXentRows = 8;  // one row per warp: Bp / 8 blocks
 
 __global__ void __launch_bounds__(256) softmax_xent_kernel(int batch, int rows, int K, const float *__restrict__ Z,
                                                            EncoderTarget tg, const int32_t *__restrict__ docs,

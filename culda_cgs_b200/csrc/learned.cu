@@ -265,10 +265,20 @@ __global__ void __launch_bounds__(kMHThreads) mh_kernel(const MHParams p) {
 }
 
 // Warm start: warp per token; the token's topic is drawn from
-// q_d(k) * phihat_wk (q_d from the doc's proposal prefix table) by inverse CDF
-// in ascending topic: lane l sums topics [l*K/32, (l+1)*K/32), a warp scan
-// finds the lane whose range holds u * total, and that lane walks its range
-// (the range's last topic if rounding leaves the walk short of the target).
+// q_d(k) * phihat_wk (q_d from the differences of the doc's proposal prefix
+// table) by inverse CDF in ascending topic.  Lanes take consecutive topics,
+// 32 at a time, so every table load is one coalesced line: a first pass sums
+// the weights, a second runs a warp scan chunk by chunk until the running sum
+// passes u * total (the last topic if rounding leaves it short).
+__device__ __forceinline__ float warm_weight(const float *__restrict__ row, const float *ph, int c, int lane,
+                                             float &carry) {
+    const float cur = __ldg(row + c + lane);
+    float prev = __shfl_up_sync(0xffffffffu, cur, 1);
+    if (lane == 0) prev = carry;
+    carry = __shfl_sync(0xffffffffu, cur, 31);
+    return (cur - prev) * ph[c + lane];
+}
+
 __global__ void __launch_bounds__(kMHThreads) warm_start_kernel(const MHParams p) {
     extern __shared__ float sm_ws[];
     const int K = p.k;
@@ -277,7 +287,6 @@ __global__ void __launch_bounds__(kMHThreads) warm_start_kernel(const MHParams p
     int *hist = reinterpret_cast<int *>(sm_ws + 2 * K);
     __shared__ int s_item;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    const int per = K >> 5;
     for (int j = tid; j < K; j += blockDim.x) inv[j] = 1.0f / ((float)p.nk[j] + p.vbeta);
     for (;;) {
         if (tid == 0) s_item = atomicAdd(p.item_counter, 1);
@@ -299,39 +308,31 @@ __global__ void __launch_bounds__(kMHThreads) warm_start_kernel(const MHParams p
                 continue;
             }
             const float *row = p.cdf + (size_t)d * K;
-            const int k0 = lane * per;
-            float prev = k0 > 0 ? __ldg(row + k0 - 1) : 0.f, s = 0.f;
-            for (int i = 0; i < per; ++i) {
-                const float c = __ldg(row + k0 + i);
-                s += (c - prev) * ph[k0 + i];
-                prev = c;
-            }
-            float incl = s;
+            float carry = 0.f, part = 0.f;
+            for (int c = 0; c < K; c += 32) part += warm_weight(row, ph, c, lane, carry);
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const float v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const float total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
             const uint64_t key = p.tok_index ? (uint64_t)__ldg(p.tok_index + t) : (uint64_t)t;
-            const float T = uniform_from_bits(philox_token(p.seed, key, 0u, kPurposeWarm)) * total;
-            const unsigned hit = __ballot_sync(0xffffffffu, incl > T);
-            const int src_lane = hit ? __ffs(hit) - 1 : 31;
-            if (lane == src_lane) {
-                float cum = incl - s;
-                prev = k0 > 0 ? __ldg(row + k0 - 1) : 0.f;
-                int pick = k0 + per - 1;
-                for (int i = 0; i < per; ++i) {
-                    const float c = __ldg(row + k0 + i);
-                    cum += (c - prev) * ph[k0 + i];
-                    prev = c;
-                    if (cum > T) {
-                        pick = k0 + i;
-                        break;
-                    }
+            const float T = uniform_from_bits(philox_token(p.seed, key, 0u, kPurposeWarm)) * part;
+            int pick = K - 1;
+            float base = 0.f;
+            carry = 0.f;
+            for (int c = 0; c < K; c += 32) {
+                float incl = warm_weight(row, ph, c, lane, carry);
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const float v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
                 }
-                p.topics_out[t] = (uint16_t)pick;
+                incl += base;
+                const unsigned hit = __ballot_sync(0xffffffffu, incl > T);
+                if (hit) {
+                    pick = c + __ffs(hit) - 1;
+                    break;
+                }
+                base = __shfl_sync(0xffffffffu, incl, 31);
             }
+            if (lane == 0) p.topics_out[t] = (uint16_t)pick;
         }
         __syncthreads();
     }

@@ -309,15 +309,11 @@ int pick_group_lanes(int requested, int k) {
     if (requested == 1 || requested == 2 || requested == 4 || requested == 8 || requested == 16 || requested == 32)
         return requested;
     // measured on the 60M-token workload (K = 1024): 4 lanes per token with the
-    // 48-register budget is the fastest variant
+    // 64-register budget is the fastest variant
     return requested == 0 ? (k <= 2048 ? 4 : 8) : -1;
 }
 
-int pick_sample_blocks(int requested, int group_lanes, int k) {
-    if (requested != 0) return requested;
-    return (k <= 2048 && sample_variant_exists(group_lanes, kSampleBlocksHigh)) ? kSampleBlocksHigh
-                                                                              : kSampleBlocksDefault;
-}
+int pick_sample_blocks(int requested) { return requested != 0 ? requested : kSampleBlocksDefault; }
 
 
 }  // namespace
@@ -501,7 +497,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: CULDA_FLAG_AUTOTUNE needs group_lanes = sample_blocks = 0");
     const int gl = pick_group_lanes(p->group_lanes, p->k);
     if (gl < 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: group_lanes=%d", p->group_lanes);
-    const int sb = pick_sample_blocks(p->sample_blocks, gl, p->k);
+    const int sb = pick_sample_blocks(p->sample_blocks);
     if (!sample_variant_exists(gl, sb))
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: no sampler for group_lanes=%d sample_blocks=%d", gl,
                     p->sample_blocks);

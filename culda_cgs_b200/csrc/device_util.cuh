@@ -5,13 +5,13 @@
 
 namespace culda {
 
-// Neumaier-compensated accumulation: s + c carries the running sum.
+// Neumaier-compensated accumulation: s + c carries the running sum.  Both
+// error terms are formed and one selected, so lanes that take different sides
+// do not diverge.
 __device__ __forceinline__ void neumaier(float &s, float &c, float x) {
     const float t = s + x;
-    if (fabsf(s) >= fabsf(x))
-        c += (s - t) + x;
-    else
-        c += (x - t) + s;
+    const float a = (s - t) + x, b = (x - t) + s;
+    c += fabsf(s) >= fabsf(x) ? a : b;
     s = t;
 }
 

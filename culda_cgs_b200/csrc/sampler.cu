@@ -115,16 +115,19 @@ __device__ __forceinline__ int dense_bucket_search(const float *qc, int K, float
 }
 
 // ------------------------------------------------------------- row walk
-// Theta entries per lane per step: one 16-byte load.  A group of 8 lanes
+// Theta entries per lane per step: two 16-byte loads.  A group of 4 lanes
 // then reads one 128-byte line of a row per step (rows start on 32 entries).
-constexpr int kLaneEntries = 4;
+constexpr int kLaneEntries = 8;
+constexpr int kLaneVecs = kLaneEntries / 4;
 
 template <int G>
 struct SampleShape {
     static constexpr int kGroups = kSampleThreads / G;
     static constexpr int kStep = kLaneEntries * G;          // entries per group step
-    static constexpr int kMaxSteps = 8 * G;                  // running sums kept per group
-    static constexpr int kPrefixFloats = kGroups * kMaxSteps;  // 1024 floats for every G
+    // running sums kept per group, enough steps for rows of up to 64 G^2
+    // entries (1024 at G = 4) to be walked once; longer rows walk again
+    static constexpr int kMaxSteps = 64 * G / kLaneEntries;
+    static constexpr int kPrefixFloats = kGroups * kMaxSteps;  // 2048 floats for every G
 };
 
 struct Step {
@@ -134,11 +137,14 @@ struct Step {
 __device__ __forceinline__ Step load_step(const ThetaEntry *__restrict__ theta, int idx, int re) {
     Step st;
     if (idx < re) {  // rows end on a multiple of 32 entries, idx on a multiple of kLaneEntries
-        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(theta + idx));
-        st.e[0] = v.x;
-        st.e[1] = v.y;
-        st.e[2] = v.z;
-        st.e[3] = v.w;
+#pragma unroll
+        for (int j = 0; j < kLaneVecs; ++j) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4 *>(theta + idx) + j);
+            st.e[4 * j] = v.x;
+            st.e[4 * j + 1] = v.y;
+            st.e[4 * j + 2] = v.z;
+            st.e[4 * j + 3] = v.w;
+        }
     } else {
 #pragma unroll
         for (int j = 0; j < kLaneEntries; ++j) st.e[j] = 0u;
@@ -267,8 +273,8 @@ __device__ __forceinline__ int draw_topic(const ThetaEntry *__restrict__ theta, 
 
 // -------------------------------------------------------------- the kernel
 // MINB resident CTAs per SM is the register budget the compiler is held to:
-// 8 -> at most 64 registers (32 warps per SM), 10 -> at most 48 (40 warps),
-// with a few spills.
+// 8 -> at most 64 registers (32 warps per SM, no spills), 10 -> at most 48
+// (40 warps, some spills).
 template <int G, int MINB>
 __global__ void __launch_bounds__(kSampleThreads, MINB) sample_kernel(const SampleParams p) {
     extern __shared__ float smem[];

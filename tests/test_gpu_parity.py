@@ -82,8 +82,7 @@ def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens, 
     seed = 1234
     with cb.LDA(c, k, 50.0 / 1024, 0.01, seed=seed, group_lanes=g, item_tokens=item_tokens,
                 sample_blocks=blocks) as m:
-        default_blocks = 10 if (k <= 2048 and g in (4, 8, 16)) else 8
-        assert m.info()["sample_blocks"] == (blocks or default_blocks)
+        assert m.info()["sample_blocks"] == (blocks or 8)
         z0 = m.topics()
         assert np.array_equal(z0, O.init_topics(c.num_tokens, k, seed))
         s0 = assert_counts_exact(m, c)

@@ -214,6 +214,7 @@ __device__ __forceinline__ float row_sum(const ThetaEntry *__restrict__ theta, c
     // the next step's entries are loaded before this step is reduced, so two
     // row loads per lane are in flight
     Step st = load_step(theta, rs + kLaneEntries * gl, re);
+#pragma unroll 2
     for (int base = rs; base < re; base += kStep, ++nst) {
         const Step nx = load_step(theta, base + kStep + kLaneEntries * gl, re);
         float p[kLaneEntries];

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -319,12 +320,10 @@ int pick_sample_blocks(int requested) { return requested != 0 ? requested : kSam
 }  // namespace
 
 // ------------------------------------------------------------- work items
-extern "C" int64_t culda_build_items(int32_t num_words, const int64_t *word_ptr, int32_t item_tokens,
-                                     culda_item *items, int64_t max_items, int32_t *num_hot) {
-    if (num_words <= 0 || !word_ptr || item_tokens <= 0) {
-        set_global_error("culda_build_items: invalid argument");
-        return CULDA_ERR_INVALID_ARG;
-    }
+// Work items, largest first (a counting sort on the token count, which is at
+// most item_tokens <= 65535; stable, so equal counts keep word order).
+std::vector<culda_item> build_items_vec(int32_t num_words, const int64_t *word_ptr, int32_t item_tokens,
+                                        int32_t *num_hot) {
     std::vector<culda_item> v;
     int32_t hot = 0;
     for (int32_t w = 0; w < num_words; ++w) {
@@ -343,8 +342,22 @@ extern "C" int64_t culda_build_items(int32_t num_words, const int64_t *word_ptr,
             ++hot;
         }
     }
-    std::stable_sort(v.begin(), v.end(), [](const culda_item &a, const culda_item &b) { return a.count > b.count; });
+    std::vector<int64_t> start((size_t)item_tokens + 2, 0);
+    for (const culda_item &x : v) start[(size_t)(item_tokens - x.count) + 1]++;
+    for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
+    std::vector<culda_item> out(v.size());
+    for (const culda_item &x : v) out[(size_t)start[(size_t)(item_tokens - x.count)]++] = x;
     if (num_hot) *num_hot = hot;
+    return out;
+}
+
+extern "C" int64_t culda_build_items(int32_t num_words, const int64_t *word_ptr, int32_t item_tokens,
+                                     culda_item *items, int64_t max_items, int32_t *num_hot) {
+    if (num_words <= 0 || !word_ptr || item_tokens <= 0 || item_tokens > 65535) {
+        set_global_error("culda_build_items: invalid argument");
+        return CULDA_ERR_INVALID_ARG;
+    }
+    const std::vector<culda_item> v = build_items_vec(num_words, word_ptr, item_tokens, num_hot);
     if (items) {
         if ((int64_t)v.size() > max_items) {
             set_global_error("culda_build_items: %zu items do not fit in %lld", v.size(), (long long)max_items);
@@ -431,13 +444,33 @@ __global__ void item_segments_kernel(culda_item *items, int num_items, const int
     }
 }
 
+// One device buffer for the set-up's temporaries (sort keys and values, scan
+// arrays, CUB scratch), carved by a bump allocator and released once: set-up
+// makes one allocation and one free instead of one pair per temporary.
+struct SetupArena {
+    char *base = nullptr;
+    size_t size = 0, used = 0;
+    template <class T>
+    T *take(size_t n) {
+        const size_t bytes = (std::max<size_t>(n, 1) * sizeof(T) + 255) & ~(size_t)255;
+        if (used + bytes > size) return nullptr;
+        T *p = reinterpret_cast<T *>(base + used);
+        used += bytes;
+        return p;
+    }
+    void reset() { used = 0; }
+};
+
+size_t arena_bytes(size_t n_items_of_4_bytes, size_t scratch) { return n_items_of_4_bytes * 4 + scratch + 16 * 256; }
+
 // Segments of the stored token order, on the device (see culda_build_segments).
-int build_segments_device(culda_ctx *ctx) {
+int build_segments_device(culda_ctx *ctx, SetupArena &arena) {
     cudaStream_t s = ctx->stream;
     const int64_t N = ctx->N;
     int32_t *mark = nullptr, *key = nullptr, *run = nullptr, *flag = nullptr, *index = nullptr;
     void *tmp = nullptr;
     size_t tmp_bytes = 0, b2 = 0;
+    arena.reset();
     int rc = CULDA_OK;
     auto grid = [](int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); };
     do {
@@ -449,11 +482,15 @@ int build_segments_device(culda_ctx *ctx) {
             break;                                                                                         \
         }                                                                                                  \
     }
-        CKS(dalloc(&mark, (size_t)N));
-        CKS(dalloc(&key, (size_t)N));
-        CKS(dalloc(&run, (size_t)N));
-        CKS(dalloc(&flag, (size_t)N + 1));
-        CKS(dalloc(&index, (size_t)N + 1));
+        mark = arena.take<int32_t>((size_t)N);
+        key = arena.take<int32_t>((size_t)N);
+        run = arena.take<int32_t>((size_t)N);
+        flag = arena.take<int32_t>((size_t)N + 1);
+        index = arena.take<int32_t>((size_t)N + 1);
+        if (!mark || !key || !run || !flag || !index) {
+            rc = fail(ctx, CULDA_ERR_OOM, "segments: set-up arena too small");
+            break;
+        }
         CKS(cudaMemsetAsync(mark, 0, sizeof(int32_t) * (size_t)N, s));
         mark_items_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, mark);
         run_key_kernel<<<grid(N), 256, 0, s>>>(N, ctx->d_doc_ids, mark, key);
@@ -461,7 +498,11 @@ int build_segments_device(culda_ctx *ctx) {
         CKS(cub::DeviceScan::InclusiveScan(nullptr, tmp_bytes, key, run, MaxOp(), (int)N, s));
         CKS(cub::DeviceScan::ExclusiveSum(nullptr, b2, flag, index, (int)N + 1, s));
         tmp_bytes = std::max(tmp_bytes, b2);
-        CKS(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 1)));
+        tmp = arena.take<char>(tmp_bytes);
+        if (!tmp) {
+            rc = fail(ctx, CULDA_ERR_OOM, "segments: set-up arena too small");
+            break;
+        }
         CKS(cub::DeviceScan::InclusiveScan(tmp, tmp_bytes, key, run, MaxOp(), (int)N, s));
         seg_flag_kernel<<<grid(N + 1), 256, 0, s>>>(N, run, flag);
         CKS(cudaGetLastError());
@@ -477,8 +518,6 @@ int build_segments_device(culda_ctx *ctx) {
         CKS(cudaStreamSynchronize(s));
 #undef CKS
     } while (0);
-    for (void *b : {(void *)mark, (void *)key, (void *)run, (void *)flag, (void *)index, tmp})
-        if (b) cudaFree(b);
     return rc;
 }
 
@@ -493,6 +532,8 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: K=%d must be a multiple of 32 in [32, 4096]", p->k);
     if (!(p->alpha > 0.f) || !(p->beta > 0.f) || !std::isfinite(p->alpha) || !std::isfinite(p->beta))
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: alpha and beta must be positive");
+    if (p->item_tokens < 0 || p->item_tokens > 65535)
+        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: item_tokens=%d outside 0..65535", p->item_tokens);
     if ((p->flags & CULDA_FLAG_AUTOTUNE) && (p->group_lanes != 0 || p->sample_blocks != 0))
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: CULDA_FLAG_AUTOTUNE needs group_lanes = sample_blocks = 0");
     const int gl = pick_group_lanes(p->group_lanes, p->k);
@@ -535,7 +576,9 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     ctx->group_lanes = gl;
     ctx->sample_blocks = sb;
     int rc = CULDA_OK;
+    SetupArena arena;  // the set-up's temporaries (sorts, segment scans)
     auto bail = [&](int code) {
+        if (arena.base) cudaFree(arena.base);
         culda_destroy(ctx);
         return code;
     };
@@ -561,6 +604,18 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     cudaStream_t s = ctx->stream;
     const int64_t N = ctx->N;
     const int32_t D = ctx->D, V = ctx->V, K = ctx->K;
+    // with CULDA_FLAG_VERBOSE, the wall time of each set-up phase (the stream
+    // is synchronised at every mark, so the marks slow set-up down a little)
+    const bool verbose = (p->flags & CULDA_FLAG_VERBOSE) != 0;
+    auto t_last = std::chrono::steady_clock::now();
+    auto mark = [&](const char *phase) {
+        if (!verbose) return;
+        cudaStreamSynchronize(s);
+        const auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "culda: set-up %-22s %8.2f ms\n", phase,
+                std::chrono::duration<double, std::milli>(now - t_last).count());
+        t_last = now;
+    };
 
     // corpus upload
     CKB(dalloc(&ctx->d_word_ptr, (size_t)V + 1));
@@ -601,58 +656,82 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     // order among equal lengths).  Neighbouring sampler groups then walk theta
     // rows of similar length.  Sampling results do not depend on this order:
     // each token's Philox stream is keyed on its input index.
+    mark("upload, doc check");
+    // one arena for the set-up's temporaries: the larger of the token-order
+    // sort (8-byte keys in and out, values), the doc-reverse sort and the
+    // segment scans (5 int arrays), plus the largest CUB scratch
+    {
+        int end_bit = 17;
+        while ((1ll << (end_bit - 16)) < (int64_t)V) ++end_bit;
+        size_t t_order = 0, t_doc = 0, t_scan = 0, t_sum = 0;
+        CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_order, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, end_bit, s));
+        CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_doc, (const int32_t *)nullptr, (int32_t *)nullptr,
+                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, 31, s));
+        CKB(cub::DeviceScan::InclusiveScan(nullptr, t_scan, (const int32_t *)nullptr, (int32_t *)nullptr, MaxOp(),
+                                           (int)N, s));
+        CKB(cub::DeviceScan::ExclusiveSum(nullptr, t_sum, (const int32_t *)nullptr, (int32_t *)nullptr, (int)N + 1,
+                                          s));
+        const size_t words = std::max<size_t>(5 * (size_t)N, 5 * ((size_t)N + 2));
+        const size_t scratch = std::max(std::max(t_order, t_doc), std::max(t_scan, t_sum));
+        arena.size = arena_bytes(words, scratch);
+        CKB(cudaMalloc((void **)&arena.base, arena.size));
+    }
+    auto arena_free = [&]() {
+        if (arena.base) cudaFree(arena.base);
+        arena.base = nullptr;
+    };
+#define CKA(call)                                                                                              \
+    do {                                                                                                       \
+        cudaError_t e_ = (call);                                                                               \
+        if (e_ != cudaSuccess) {                                                                               \
+            arena_free();                                                                                      \
+            CKB(e_);                                                                                           \
+        }                                                                                                      \
+    } while (0)
     if (!(p->flags & CULDA_FLAG_NO_REORDER)) {
-        uint64_t *keys = nullptr, *keys_out = nullptr;
-        int32_t *vals = nullptr, *ids2 = nullptr;
-        CKB(dalloc(&keys, (size_t)N));
-        CKB(dalloc(&keys_out, (size_t)N));
-        CKB(dalloc(&vals, (size_t)N));
-        CKB(dalloc(&ctx->d_tok_index, (size_t)N));
-        CKB(launch_order_keys(V, N, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, keys, s));
-        CKB(launch_iota(N, vals, s));
+        arena.reset();
+        uint64_t *keys = arena.take<uint64_t>((size_t)N), *keys_out = arena.take<uint64_t>((size_t)N);
+        int32_t *vals = arena.take<int32_t>((size_t)N), *ids2 = nullptr;
         int end_bit = 17;
         while ((1ll << (end_bit - 16)) < (int64_t)V) ++end_bit;
         size_t tmp_bytes = 0;
-        CKB(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
+        CKA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
                                             end_bit, s));
-        void *tmp = nullptr;
-        CKB(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 1)));
-        CKB(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
+        void *tmp = arena.take<char>(tmp_bytes);
+        if (!keys || !keys_out || !vals || !tmp) CKA(cudaErrorMemoryAllocation);
+        CKA(dalloc(&ctx->d_tok_index, (size_t)N));
+        CKA(launch_order_keys(V, N, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, keys, s));
+        CKA(launch_iota(N, vals, s));
+        CKA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
                                             end_bit, s));
-        CKB(dalloc(&ids2, (size_t)N));
-        CKB(launch_gather<int32_t>(N, ctx->d_tok_index, ctx->d_doc_ids, ids2, s));
-        CKB(cudaStreamSynchronize(s));
-        cudaFree(tmp);
-        cudaFree(keys);
-        cudaFree(keys_out);
-        cudaFree(vals);
+        CKA(dalloc(&ids2, (size_t)N));
+        CKA(launch_gather<int32_t>(N, ctx->d_tok_index, ctx->d_doc_ids, ids2, s));
+        CKA(cudaStreamSynchronize(s));
         cudaFree(ctx->d_doc_ids);
         ctx->d_doc_ids = ids2;
     }
 
+    mark("token order sort");
     // doc-reverse index: stable radix sort of stored token positions by doc id
     // (the reference builds it on the host, doc_chunk.cpp:225-255)
     {
-        CKB(dalloc(&ctx->d_doc_tok, (size_t)N));
-        int32_t *keys_out = nullptr, *vals_in = nullptr;
-        CKB(dalloc(&keys_out, (size_t)N));
-        CKB(dalloc(&vals_in, (size_t)N));
-        CKB(launch_iota(N, vals_in, s));
+        arena.reset();
+        CKA(dalloc(&ctx->d_doc_tok, (size_t)N));
+        int32_t *keys_out = arena.take<int32_t>((size_t)N), *vals_in = arena.take<int32_t>((size_t)N);
         int end_bit = 1;
         while ((1ll << end_bit) < (int64_t)D) ++end_bit;
         size_t tmp_bytes = 0;
-        CKB(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok,
+        CKA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok,
                                             (int)N, 0, end_bit, s));
-        void *tmp = nullptr;
-        CKB(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 1)));
-        CKB(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok, (int)N,
+        void *tmp = arena.take<char>(tmp_bytes);
+        if (!keys_out || !vals_in || !tmp) CKA(cudaErrorMemoryAllocation);
+        CKA(launch_iota(N, vals_in, s));
+        CKA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok, (int)N,
                                             0, end_bit, s));
-        CKB(cudaStreamSynchronize(s));
-        cudaFree(tmp);
-        cudaFree(keys_out);
-        cudaFree(vals_in);
     }
 
+    mark("doc-reverse sort");
     // theta layout: capacity roundup32(min(L_d, K)) per doc (model_theta.cpp:50-56)
     ctx->h_doc_ptr.assign(c->doc_ptr, c->doc_ptr + D + 1);
     ctx->h_max_ia.resize((size_t)D + 1);
@@ -679,18 +758,19 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     CKB(dalloc(&ctx->d_rows, (size_t)D));
     CKB(cudaMemcpyAsync(ctx->d_rows, rows.data(), sizeof(int2) * (size_t)D, cudaMemcpyHostToDevice, s));
 
-    // docs longest first for the theta rebuild's warps
+    // docs longest first for the theta rebuild's warps: a counting sort on
+    // the length (below 65536), stable in doc id
     {
-        std::vector<int32_t> order((size_t)D);
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
-            return c->doc_ptr[a + 1] - c->doc_ptr[a] > c->doc_ptr[b + 1] - c->doc_ptr[b];
-        });
+        std::vector<int32_t> order((size_t)D), start(65537, 0);
+        for (int32_t d = 0; d < D; ++d) start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d])) + 1]++;
+        for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+        for (int32_t d = 0; d < D; ++d) order[(size_t)start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d]))]++] = d;
         CKB(dalloc(&ctx->d_doc_order, (size_t)D));
         CKB(cudaMemcpyAsync(ctx->d_doc_order, order.data(), sizeof(int32_t) * (size_t)D, cudaMemcpyHostToDevice, s));
         CKB(cudaStreamSynchronize(s));
     }
 
+    mark("theta layout, order");
     // grids
     const int sms = num_sms(ctx->device);
     int sbps = sample_blocks_per_sm(K, gl, sb);
@@ -708,13 +788,13 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         if (it <= 0) it = std::max<int64_t>(1024, std::min<int64_t>(65535, N / ((int64_t)sms * sbps * 4)));
         ctx->item_tokens = (int)it;
         int32_t nhot = 0;
-        const int64_t n_items = culda_build_items(V, c->word_ptr, ctx->item_tokens, nullptr, 0, &nhot);
+        const std::vector<culda_item> items = build_items_vec(V, c->word_ptr, ctx->item_tokens, &nhot);
+        const int64_t n_items = (int64_t)items.size();
         if (n_items <= 0 || n_items >= INT32_MAX) {
             fail(ctx, CULDA_ERR_FORMAT, "culda_create: no tokens to sample");
             return bail(CULDA_ERR_FORMAT);
         }
-        std::vector<culda_item> items((size_t)n_items), hot;
-        culda_build_items(V, c->word_ptr, ctx->item_tokens, items.data(), n_items, &nhot);
+        std::vector<culda_item> hot;
         for (const culda_item &x : items)
             if (x.hot >= 0) hot.push_back(x);
         ctx->num_items = (int32_t)n_items;
@@ -731,7 +811,10 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         CKB(cudaStreamSynchronize(s));
     }
     ctx->sample_grid = std::max(1, std::min(ctx->num_items, sms * sbps));
-    rc = build_segments_device(ctx);
+    mark("work items");
+    rc = build_segments_device(ctx, arena);
+    arena_free();
+#undef CKA
     if (rc) return bail(rc);
 
     CKB(dalloc(&ctx->d_counter, 64));
@@ -744,6 +827,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     const uint32_t one = 1;
     CKB(cudaMemcpyAsync(ctx->d_iter, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
 
+    mark("segments");
     // topics: Philox init, then the initial counts (SingleChunkSingleGPU.h:24-41)
     CKB(dalloc(&ctx->d_z[0], (size_t)N));
     CKB(dalloc(&ctx->d_z[1], (size_t)N));
@@ -765,8 +849,10 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
             ctx->tune_pending = true;
         }
     }
+    mark("init topics, counts");
     rc = build_graphs(ctx);
     if (rc) return bail(rc);
+    mark("graph capture");
     if (p->flags & CULDA_FLAG_VERBOSE)
         fprintf(stderr,
                 "culda: D=%d V=%d N=%lld K=%d items=%d hot_words=%d hot_items=%d item_tokens=%d theta_cap=%lld "

@@ -146,7 +146,7 @@ typedef struct culda_params {
     uint64_t seed;        /* Philox key for init and sampling */
     int32_t device;       /* CUDA device ordinal */
     int32_t group_lanes;  /* lanes per token in the sampler: 0 = auto, else 1,2,4,8,16,32 */
-    int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto */
+    int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto, at most 65535 */
     int32_t flags;        /* CULDA_FLAG_* */
     int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (8),
                               8 (<= 64 registers), or 10 (<= 48 registers; group_lanes 4, 8, 16) */

@@ -149,6 +149,8 @@ SIGNATURES = {
     "culda_iterate_mh": (C.c_int, [C.c_void_p, i32, i32, P(IterStats)]),
     "culda_mh_snapshot": (C.c_int, [C.c_void_p, u32, i32, C.c_void_p]),
     "culda_set_frozen_phi": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "culda_next_iteration": (u32, [C.c_void_p]),
+    "culda_set_iteration": (C.c_int, [C.c_void_p, u32]),
     "culda_warm_start": (C.c_int, [C.c_void_p]),
 }
 

@@ -1084,6 +1084,17 @@ extern "C" int culda_get_info(const culda_ctx *ctx, culda_info *info) {
 
 extern "C" const char *culda_last_error(const culda_ctx *ctx) { return ctx ? ctx->err.c_str() : global_error(); }
 
+extern "C" uint32_t culda_next_iteration(const culda_ctx *ctx) { return ctx ? ctx->next_iteration : 0u; }
+
+extern "C" int culda_set_iteration(culda_ctx *ctx, uint32_t iteration) {
+    if (!ctx || iteration == 0u) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_set_iteration: invalid argument");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(ctx->d_iter, &iteration, sizeof(uint32_t), cudaMemcpyHostToDevice));
+    ctx->next_iteration = iteration;
+    return CULDA_OK;
+}
+
 extern "C" void culda_destroy(culda_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);

@@ -52,6 +52,7 @@ class LDA:
         self.num_tokens = corpus.num_tokens
         self.num_docs = corpus.num_docs
         self.num_words = corpus.num_words
+        self.seed = int(seed)
         p = _ffi.Params(self.k, alpha, beta, seed, device, group_lanes, item_tokens, flags, sample_blocks)
         self._ctx = C.c_void_p()
         check(lib().culda_create(corpus.c_ptr, C.byref(p), C.byref(self._ctx)))
@@ -128,6 +129,29 @@ class LDA:
         z = np.ascontiguousarray(z, dtype=np.uint16)
         assert z.shape == (self.num_tokens,)
         self._check(lib().culda_set_topics(self._ctx, _u16p(z)))
+
+    # ------------------------------------------------- checkpoint / resume
+    @property
+    def next_iteration(self) -> int:
+        return int(lib().culda_next_iteration(self._ctx))
+
+    def set_iteration(self, iteration: int) -> None:
+        self._check(lib().culda_set_iteration(self._ctx, int(iteration)))
+
+    def save(self, path) -> None:
+        """The chain's state (topics in input order, next iteration, settings)
+        as an .npz file."""
+        np.savez_compressed(path, topics=self.topics(), next_iteration=self.next_iteration, k=self.k,
+                            alpha=self.alpha, beta=self.beta, seed=self.seed, num_tokens=self.num_tokens)
+
+    def restore(self, path) -> None:
+        """Resume a chain saved by save() on the same corpus and settings."""
+        f = np.load(path)
+        if int(f["num_tokens"]) != self.num_tokens or int(f["k"]) != self.k or int(f["seed"]) != self.seed or \
+                float(f["alpha"]) != self.alpha or float(f["beta"]) != self.beta:
+            raise ValueError("checkpoint does not match this corpus and these settings")
+        self.set_topics(f["topics"])
+        self.set_iteration(int(f["next_iteration"]))
 
     def phi(self, dense: bool = True) -> tuple[np.ndarray | None, np.ndarray]:
         nk = np.empty(self.k, dtype=np.int32)

@@ -198,6 +198,17 @@ int culda_iterate(culda_ctx *ctx, int n, culda_iter_stats *stats);
 /* Replace all topics from a host array and rebuild the counts. */
 int culda_set_topics(culda_ctx *ctx, const uint16_t *topics);
 
+/* Checkpoint and resume (no reference counterpart; the reference saves no
+ * usable model state, model_phi.cpp:161-189): the state of a chain is its
+ * topics (culda_get_topics) and the number of its next iteration, which keys
+ * the Philox draws.  A context created with the same corpus, K, alpha, beta
+ * and seed, given those topics (culda_set_topics) and that iteration number,
+ * continues with exactly the draws the original chain would have made.
+ * culda_next_iteration returns the number (1-based), culda_set_iteration sets
+ * it (>= 1). */
+uint32_t culda_next_iteration(const culda_ctx *ctx);
+int culda_set_iteration(culda_ctx *ctx, uint32_t iteration);
+
 /* Copy state back (reference: DocChunk::toCPU, ModelPhi::MasterGPUToCPU,
  * ModelTheta::toCPU, SingleChunkSingleGPU.h:138-148).  Any pointer may be NULL. */
 int culda_get_topics(culda_ctx *ctx, uint16_t *topics);

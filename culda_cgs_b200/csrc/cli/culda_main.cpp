@@ -7,7 +7,10 @@
 // Extra options (off by default, so parsers of the reference's output keep
 // working): -seed <n> (Philox key, default 1), -G <lanes> (sampler lanes per
 // token), -j (print the FP64 joint log-likelihood on a separate line after
-// each iteration), -z <file> (write the final topics as int16).
+// each iteration), -z <file> (write the final topics as int16).  -o <prefix>,
+// accepted and unused by the reference, writes <prefix>.topwords: each
+// topic's token count and its 20 most frequent words.
+#include <algorithm>
 #include <cctype>
 #include <chrono>
 #include <cstdio>
@@ -167,6 +170,35 @@ int main(int argc, char **argv) {
             rc = CULDA_ERR_IO;
         }
         if (f) fclose(f);
+    }
+    // -o: the model summary the reference's commented-out saveWord
+    // (model_phi.cpp:283-329) would have written: per topic its token count
+    // and its 20 most frequent words (word id:count)
+    if (rc == CULDA_OK && !arg.outputFilePrefix.empty()) {
+        const int K = arg.k, V = corpus->num_words;
+        std::vector<int32_t> phi((size_t)V * K), nk((size_t)K);
+        rc = culda_get_phi(ctx, phi.data(), nk.data());
+        const std::string path = arg.outputFilePrefix + ".topwords";
+        FILE *f = rc == CULDA_OK ? fopen(path.c_str(), "w") : nullptr;
+        if (!f) {
+            fprintf(stderr, "Error: writing %s failed\n", path.c_str());
+            rc = CULDA_ERR_IO;
+        } else {
+            std::vector<int32_t> idx((size_t)V);
+            for (int k = 0; k < K; ++k) {
+                for (int w = 0; w < V; ++w) idx[(size_t)w] = w;
+                const int top = std::min(20, V);
+                std::partial_sort(idx.begin(), idx.begin() + top, idx.end(), [&](int32_t a, int32_t b) {
+                    const int32_t ca = phi[(size_t)a * K + k], cb = phi[(size_t)b * K + k];
+                    return ca != cb ? ca > cb : a < b;
+                });
+                fprintf(f, "topic %d tokens %d:", k, nk[(size_t)k]);
+                for (int i = 0; i < top && phi[(size_t)idx[(size_t)i] * K + k] > 0; ++i)
+                    fprintf(f, " %d:%d", idx[(size_t)i], phi[(size_t)idx[(size_t)i] * K + k]);
+                fprintf(f, "\n");
+            }
+            fclose(f);
+        }
     }
     printf("\n");
     culda_destroy(ctx);

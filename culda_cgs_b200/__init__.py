@@ -6,9 +6,9 @@ over it that mirrors the reference's host interface (Document, Argument,
 LDATrain).
 """
 from ._ffi import CULDA_FLAG_AUTOTUNE, CULDA_FLAG_NO_GRAPH, CULDA_FLAG_NO_REORDER, CULDA_FLAG_VERBOSE, CuldaError, lib, library_path
-from .corpus import BorrowedCorpus, Corpus, Document, GenConfig
+from .corpus import BorrowedCorpus, Corpus, Document, GenConfig, format_text
 from .encoder import Encoder
 from .lda import LDA, Argument, LDATrain
 
-__all__ = ["CuldaError", "lib", "library_path", "Corpus", "BorrowedCorpus", "Document", "GenConfig", "LDA",
-           "Argument", "LDATrain", "Encoder"]
+__all__ = ["CuldaError", "lib", "library_path", "Corpus", "BorrowedCorpus", "Document", "GenConfig", "format_text",
+           "LDA", "Argument", "LDATrain", "Encoder"]

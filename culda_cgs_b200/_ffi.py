@@ -34,6 +34,10 @@ class Corpus(C.Structure):
                 ("word_ptr", P(i64)), ("doc_ids", P(i32)), ("word_label", P(i32)), ("owned", i32)]
 
 
+class Vocab(C.Structure):
+    _fields_ = [("num_words", i32), ("offsets", P(i64)), ("bytes", C.c_void_p)]
+
+
 class GenParams(C.Structure):
     _fields_ = [("num_words", i32), ("num_topics", i32), ("num_docs", i32), ("len_law", i32), ("zipf_s", f64),
                 ("word_conc", f64), ("doc_conc", f64), ("len_a", f64), ("len_b", f64), ("len_min", i32),
@@ -105,6 +109,10 @@ SIGNATURES = {
     "culda_corpus_write_text": (C.c_int, [P(Corpus), C.c_char_p]),
     "culda_corpus_free": (None, [P(Corpus)]),
     "culda_corpus_doc_tokens": (C.c_int, [P(Corpus), P(i32)]),
+    "culda_vocab_free": (None, [P(Vocab)]),
+    "culda_corpus_from_text": (C.c_int, [C.c_char_p, i32, P(P(Corpus)), P(P(Vocab))]),
+    "culda_format_write": (C.c_int, [P(Corpus), P(Vocab), C.c_char_p, C.c_int]),
+    "culda_format_text": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, i32]),
     "culda_create": (C.c_int, [P(Corpus), P(Params), P(C.c_void_p)]),
     "culda_iterate": (C.c_int, [C.c_void_p, C.c_int, P(IterStats)]),
     "culda_set_topics": (C.c_int, [C.c_void_p, P(u16)]),

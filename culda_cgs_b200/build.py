@@ -5,6 +5,7 @@ objects and binaries travel with the source tree:
 
     culda_cgs_b200/libculda_b200.so   CUDA kernels + C ABI (include/culda_b200.h)
     culda_cgs_b200/bin/culda          C++ host with the reference's CLI
+    culda_cgs_b200/bin/format         C++ host with the reference's preprocessing tool
     oracle/liboracle.so               host FP64 oracle + OpenMP CPU baseline (tests/bench only)
     oracle/_ref/...                   the reference's own build (only where its sources exist)
 """
@@ -21,6 +22,7 @@ PKG = ROOT / "culda_cgs_b200"
 CSRC = PKG / "csrc"
 LIB = PKG / "libculda_b200.so"
 CLI = PKG / "bin" / "culda"
+FORMAT_CLI = PKG / "bin" / "format"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # portable host ISA: the library is built here and run on the GPU hosts
 HOST_ARCH = "-march=x86-64-v2"
@@ -52,7 +54,7 @@ def _stale(target: Path, sources: list[Path]) -> bool:
 
 
 def library_sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu")) + [CSRC / "corpus.cpp"]
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
 def build_library(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> Path:
@@ -72,22 +74,30 @@ def build_library(verbose: bool = False, force: bool = False, ptxas_info: bool =
     return LIB
 
 
-def build_cli(verbose: bool = False, force: bool = False) -> Path:
-    src = CSRC / "cli" / "culda_main.cpp"
+def _build_host_tool(src: Path, exe: Path, verbose: bool, force: bool) -> Path:
     if not src.exists():
-        return CLI
-    if not force and not _stale(CLI, [src, LIB, ROOT / "include" / "culda_b200.h"]):
-        return CLI
-    CLI.parent.mkdir(parents=True, exist_ok=True)
-    cmd = ["g++", "-O2", "-std=c++17", HOST_ARCH, "-I", str(ROOT / "include"), "-o", str(CLI), str(src),
+        return exe
+    if not force and not _stale(exe, [src, LIB, ROOT / "include" / "culda_b200.h"]):
+        return exe
+    exe.parent.mkdir(parents=True, exist_ok=True)
+    cmd = ["g++", "-O2", "-std=c++17", HOST_ARCH, "-I", str(ROOT / "include"), "-o", str(exe), str(src),
            "-L", str(PKG), "-lculda_b200", "-Wl,-rpath,$ORIGIN/.."]
     _run(cmd, verbose)
-    return CLI
+    return exe
+
+
+def build_cli(verbose: bool = False, force: bool = False) -> Path:
+    return _build_host_tool(CSRC / "cli" / "culda_main.cpp", CLI, verbose, force)
+
+
+def build_format_cli(verbose: bool = False, force: bool = False) -> Path:
+    return _build_host_tool(CSRC / "cli" / "format_main.cpp", FORMAT_CLI, verbose, force)
 
 
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_library(verbose, force)
     build_cli(verbose, force)
+    build_format_cli(verbose, force)
     sys.path.insert(0, str(ROOT))
     from oracle import build_oracle  # the checker is built beside the product, never linked into it
 

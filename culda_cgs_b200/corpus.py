@@ -44,6 +44,7 @@ class Corpus:
 
     def __init__(self, ptr: C.POINTER(_ffi.Corpus)):
         self._ptr = ptr
+        self._vocab = None  # culda_vocab of a corpus read from text
         c = ptr.contents
         self.num_docs = int(c.num_docs)
         self.num_words = int(c.num_words)
@@ -64,12 +65,40 @@ class Corpus:
         return cls(out)
 
     @classmethod
+    def from_text(cls, path: str, threads: int = 0) -> "Corpus":
+        """Parse a text corpus, one document per line: a title field, then the
+        document's tokens (src_format/format.cpp:64-90).  Word ids follow first
+        appearance; the token strings are in `vocab`."""
+        out = C.POINTER(_ffi.Corpus)()
+        voc = C.POINTER(_ffi.Vocab)()
+        check(lib().culda_corpus_from_text(str(path).encode(), int(threads), C.byref(out), C.byref(voc)))
+        c = cls(out)
+        c._vocab = voc
+        return c
+
+    @property
+    def vocab(self) -> list[str] | None:
+        """Token strings by word id (None unless the corpus was read from text);
+        bytes that are not UTF-8 are kept as surrogate escapes."""
+        if not self._vocab:
+            return None
+        v = self._vocab.contents
+        off = np.ctypeslib.as_array(v.offsets, shape=(v.num_words + 1,))
+        raw = C.string_at(v.bytes, int(off[-1])) if off[-1] else b""
+        return [raw[off[i]:off[i + 1]].decode("utf-8", "surrogateescape") for i in range(v.num_words)]
+
+    @classmethod
     def from_arrays(cls, doc_ptr, word_ptr, doc_ids) -> "BorrowedCorpus":
         return BorrowedCorpus(doc_ptr, word_ptr, doc_ids)
 
     # --- I/O
     def write(self, prefix: str, num_chunks: int = 1) -> None:
-        check(lib().culda_corpus_write(self._ptr, str(prefix).encode(), int(num_chunks)))
+        """The src_format files; `.vocab` holds the token strings of a corpus
+        read from text, else "w<label>" names."""
+        if self._vocab:
+            check(lib().culda_format_write(self._ptr, self._vocab, str(prefix).encode(), int(num_chunks)))
+        else:
+            check(lib().culda_corpus_write(self._ptr, str(prefix).encode(), int(num_chunks)))
 
     def write_text(self, path: str) -> None:
         check(lib().culda_corpus_write_text(self._ptr, str(path).encode()))
@@ -138,12 +167,22 @@ class Corpus:
         if self._ptr:
             lib().culda_corpus_free(self._ptr)
             self._ptr = None
+        if getattr(self, "_vocab", None):
+            lib().culda_vocab_free(self._vocab)
+            self._vocab = None
 
     def __del__(self):
         try:
             self.close()
         except Exception:
             pass
+
+
+def format_text(in_path: str, out_prefix: str, num_chunks: int = 1, threads: int = 0) -> None:
+    """The reference's `format input output_prefix numChunks` tool
+    (src_format/format.cpp:19-165): text corpus in, the five word-first files
+    out, byte-identical, parsed on `threads` host threads (0 = all)."""
+    check(lib().culda_format_text(str(in_path).encode(), str(out_prefix).encode(), int(num_chunks), int(threads)))
 
 
 class BorrowedCorpus(Corpus):

@@ -42,7 +42,7 @@ void set_global_error(const char *fmt, ...) {
 const char *global_error() { return g_error.c_str(); }
 
 // ------------------------------------------------------------ file reading
-static bool read_file(const std::string &path, std::vector<char> &buf) {
+bool read_file_bytes(const std::string &path, std::vector<char> &buf) {
     FILE *f = fopen(path.c_str(), "rb");
     if (!f) return false;
     if (fseek(f, 0, SEEK_END) != 0) {
@@ -179,12 +179,12 @@ extern "C" int culda_corpus_load(const char *prefix, int num_chunks, culda_corpu
         fclose(f);
     }
     std::vector<int64_t> doc_end, chunk_end, word_end;
-    if (!read_file(pre + ".doc.idx", buf)) {
+    if (!read_file_bytes(pre + ".doc.idx", buf)) {
         set_global_error("File %s.doc.idx open failed", prefix);
         return CULDA_ERR_IO;
     }
     parse_pairs(buf, doc_end);
-    if (!read_file(pre + ".chunk", buf)) {
+    if (!read_file_bytes(pre + ".chunk", buf)) {
         set_global_error("File %s.chunk open failed", prefix);
         return CULDA_ERR_IO;
     }
@@ -193,13 +193,13 @@ extern "C" int culda_corpus_load(const char *prefix, int num_chunks, culda_corpu
         set_global_error("Error: numChunks(%d) does not match the chunk file", num_chunks);
         return CULDA_ERR_FORMAT;
     }
-    if (!read_file(pre + ".word.idx", buf)) {
+    if (!read_file_bytes(pre + ".word.idx", buf)) {
         set_global_error("File %s.word.idx open failed", prefix);
         return CULDA_ERR_IO;
     }
     parse_pairs(buf, word_end);
     std::vector<char> data;
-    if (!read_file(pre + ".word.data", data)) {
+    if (!read_file_bytes(pre + ".word.data", data)) {
         set_global_error("File %s.word.data open failed", prefix);
         return CULDA_ERR_IO;
     }
@@ -246,56 +246,132 @@ extern "C" int culda_corpus_load(const char *prefix, int num_chunks, culda_corpu
 // ---------------------------------------------------------------- writing
 namespace {
 
-struct OutFile {
-    FILE *f = nullptr;
-    std::vector<char> buf;
-    explicit OutFile(const std::string &path) {
-        f = fopen(path.c_str(), "wb");
-        if (f) {
-            buf.resize(1 << 22);
-            setvbuf(f, buf.data(), _IOFBF, buf.size());
-        }
-    }
+// Buffered output file with a decimal integer formatter (the text files hold
+// millions of "id value" lines).
+class OutFile {
+  public:
+    explicit OutFile(const std::string &path) : f_(fopen(path.c_str(), "wb")) { buf_.reserve(kBuf); }
     ~OutFile() {
-        if (f) fclose(f);
+        if (f_) fclose(f_);
     }
-    bool ok() const { return f != nullptr; }
+    bool ok() const { return f_ != nullptr; }
+    void put(const char *p, size_t n) {
+        if (buf_.size() + n > kBuf) flush();
+        if (n > kBuf) {
+            if (fwrite(p, 1, n, f_) != n) bad_ = true;
+            return;
+        }
+        buf_.insert(buf_.end(), p, p + n);
+    }
+    void put(char ch) { put(&ch, 1); }
+    void put_int(int64_t v) {
+        char tmp[24];
+        char *e = tmp + sizeof(tmp), *p = e;
+        uint64_t u = v < 0 ? 0 - (uint64_t)v : (uint64_t)v;
+        do {
+            *--p = char('0' + u % 10);
+            u /= 10;
+        } while (u);
+        if (v < 0) *--p = '-';
+        put(p, (size_t)(e - p));
+    }
+    // "a b\n", the `out << a << " " << b << endl` lines of the reference's files
+    void pair_line(int64_t a, int64_t b) {
+        put_int(a);
+        put(' ');
+        put_int(b);
+        put('\n');
+    }
     bool close() {
-        bool good = f && ferror(f) == 0;
-        if (f && fclose(f) != 0) good = false;
-        f = nullptr;
+        if (!f_) return false;
+        flush();
+        bool good = !bad_ && ferror(f_) == 0;
+        if (fclose(f_) != 0) good = false;
+        f_ = nullptr;
         return good;
+    }
+
+  private:
+    static constexpr size_t kBuf = 1 << 22;
+    FILE *f_;
+    std::vector<char> buf_;
+    bool bad_ = false;
+    void flush() {
+        if (!buf_.empty() && fwrite(buf_.data(), 1, buf_.size(), f_) != buf_.size()) bad_ = true;
+        buf_.clear();
     }
 };
 
-}  // namespace
-
-extern "C" int culda_corpus_write(const culda_corpus *c, const char *prefix, int num_chunks) {
-    if (!c || !prefix) {
-        set_global_error("culda_corpus_write: null argument");
+// The checks the writer needs: consistent prefixes and doc ids in range.
+// Unlike validate_corpus it accepts empty corpora and any token count, as the
+// reference's tool does.
+int check_for_writing(const culda_corpus *c, const culda_vocab *v) {
+    if (c->num_docs < 0 || c->num_words < 0 || c->num_tokens < 0 || !c->doc_ptr || !c->word_ptr ||
+        (c->num_tokens > 0 && !c->doc_ids)) {
+        set_global_error("corpus: negative sizes or missing arrays");
         return CULDA_ERR_INVALID_ARG;
     }
-    int rc = validate_corpus(c);
+    if (v && (v->num_words != c->num_words || !v->offsets || (v->offsets[v->num_words] > 0 && !v->bytes))) {
+        set_global_error("vocabulary: %d words for a corpus of %d", v->num_words, c->num_words);
+        return CULDA_ERR_INVALID_ARG;
+    }
+    if (c->doc_ptr[0] != 0 || c->word_ptr[0] != 0 || c->doc_ptr[c->num_docs] != c->num_tokens ||
+        c->word_ptr[c->num_words] != c->num_tokens) {
+        set_global_error("corpus: doc/word index totals do not match %lld tokens", (long long)c->num_tokens);
+        return CULDA_ERR_FORMAT;
+    }
+    for (int32_t w = 0; w < c->num_words; ++w)
+        if (c->word_ptr[w + 1] < c->word_ptr[w]) {
+            set_global_error("corpus: word index decreases at word %d", w);
+            return CULDA_ERR_FORMAT;
+        }
+    for (int64_t t = 0; t < c->num_tokens; ++t)
+        if (c->doc_ids[t] < 0 || c->doc_ids[t] >= c->num_docs) {
+            set_global_error("corpus: token %lld has doc id %d outside [0, %d)", (long long)t, c->doc_ids[t],
+                             c->num_docs);
+            return CULDA_ERR_FORMAT;
+        }
+    return CULDA_OK;
+}
+
+}  // namespace
+
+extern "C" int culda_format_write(const culda_corpus *c, const culda_vocab *vocab, const char *prefix,
+                                  int num_chunks) {
+    if (!c || !prefix) {
+        set_global_error("culda_format_write: null argument");
+        return CULDA_ERR_INVALID_ARG;
+    }
+    int rc = check_for_writing(c, vocab);
     if (rc != CULDA_OK) return rc;
     if (num_chunks <= 1) num_chunks = 1;  // src_format/format.cpp:27-28
     std::string pre(prefix);
     {
-        OutFile f(pre + ".vocab");
+        OutFile f(pre + ".vocab");  // src_format/format.cpp:96-99
         if (!f.ok()) {
             set_global_error("%s.vocab open failed", prefix);
             return CULDA_ERR_IO;
         }
-        for (int32_t w = 0; w < c->num_words; ++w)
-            fprintf(f.f, "w%d %d\n", c->word_label ? c->word_label[w] : w, w);
+        for (int32_t w = 0; w < c->num_words; ++w) {
+            if (vocab) {
+                f.put(vocab->bytes + vocab->offsets[w], (size_t)(vocab->offsets[w + 1] - vocab->offsets[w]));
+            } else {
+                f.put('w');
+                f.put_int(c->word_label ? c->word_label[w] : w);
+            }
+            f.put(' ');
+            f.put_int(w);
+            f.put('\n');
+        }
         if (!f.close()) return CULDA_ERR_IO;
     }
     {
-        OutFile f(pre + ".doc.idx");
+        OutFile f(pre + ".doc.idx");  // src_format/format.cpp:86
         if (!f.ok()) {
             set_global_error("%s.doc.idx open failed", prefix);
             return CULDA_ERR_IO;
         }
-        for (int32_t d = 0; d < c->num_docs; ++d) fprintf(f.f, "%d %lld\n", d, (long long)c->doc_ptr[d + 1]);
+        for (int32_t d = 0; d < c->num_docs; ++d) f.pair_line(d, c->doc_ptr[d + 1]);
         if (!f.close()) return CULDA_ERR_IO;
     }
     // Doc -> chunk map by equal token counts (src_format/format.cpp:107-132).
@@ -316,11 +392,14 @@ extern "C" int culda_corpus_write(const culda_corpus *c, const char *prefix, int
                 ++d;
                 if (sz >= per_chunk) break;
             }
-            fprintf(f.f, "%d %d\n", ch, d);
+            f.pair_line(ch, d);
         }
         chunk_start[num_chunks] = d;
         if (!f.close()) return CULDA_ERR_IO;
     }
+    // Per chunk, every word's entries for the chunk's docs: a word's doc list
+    // is ascending and a chunk is a doc range, so they are one contiguous run
+    // (src_format/data_chunk.h:49-67 writes the same bytes from per-chunk lists).
     for (int ch = 0; ch < num_chunks; ++ch) {
         std::string idx_name = pre + ".word.idx", data_name = pre + ".word.data";
         if (num_chunks > 1) {
@@ -329,29 +408,34 @@ extern "C" int culda_corpus_write(const culda_corpus *c, const char *prefix, int
         }
         OutFile fi(idx_name), fd(data_name);
         if (!fi.ok() || !fd.ok()) {
-            set_global_error("%s open failed", idx_name.c_str());
+            set_global_error("%s open failed", (fi.ok() ? data_name : idx_name).c_str());
             return CULDA_ERR_IO;
         }
-        int32_t d0 = chunk_start[ch], d1 = chunk_start[ch + 1];
+        const int32_t d0 = chunk_start[ch], d1 = chunk_start[ch + 1];
         int64_t off = 0;
-        std::vector<int32_t> tmp;
         for (int32_t w = 0; w < c->num_words; ++w) {
             const int32_t *b = c->doc_ids + c->word_ptr[w], *e = c->doc_ids + c->word_ptr[w + 1];
-            if (num_chunks == 1) {
-                off += e - b;
-                if (e > b) fwrite(b, sizeof(int32_t), (size_t)(e - b), fd.f);
-            } else {
-                tmp.clear();
-                for (const int32_t *p = b; p < e; ++p)
-                    if (*p >= d0 && *p < d1) tmp.push_back(*p);
-                off += (int64_t)tmp.size();
-                if (!tmp.empty()) fwrite(tmp.data(), sizeof(int32_t), tmp.size(), fd.f);
+            if (num_chunks > 1) {
+                b = std::lower_bound(b, e, d0);
+                e = std::lower_bound(b, e, d1);
             }
-            fprintf(fi.f, "%d %lld\n", w, (long long)off);
+            off += e - b;
+            if (e > b) fd.put((const char *)b, (size_t)(e - b) * sizeof(int32_t));
+            fi.pair_line(w, off);
         }
         if (!fi.close() || !fd.close()) return CULDA_ERR_IO;
     }
     return CULDA_OK;
+}
+
+extern "C" int culda_corpus_write(const culda_corpus *c, const char *prefix, int num_chunks) {
+    if (!c || !prefix) {
+        set_global_error("culda_corpus_write: null argument");
+        return CULDA_ERR_INVALID_ARG;
+    }
+    int rc = validate_corpus(c);
+    if (rc != CULDA_OK) return rc;
+    return culda_format_write(c, nullptr, prefix, num_chunks);
 }
 
 extern "C" int culda_corpus_write_text(const culda_corpus *c, const char *path) {
@@ -371,10 +455,13 @@ extern "C" int culda_corpus_write_text(const culda_corpus *c, const char *path) 
         return CULDA_ERR_IO;
     }
     for (int32_t d = 0; d < c->num_docs; ++d) {
-        fprintf(f.f, "d%d", d);
-        for (int64_t i = c->doc_ptr[d]; i < c->doc_ptr[d + 1]; ++i)
-            fprintf(f.f, " w%d", c->word_label ? c->word_label[words[i]] : words[i]);
-        fputc('\n', f.f);
+        f.put('d');
+        f.put_int(d);
+        for (int64_t i = c->doc_ptr[d]; i < c->doc_ptr[d + 1]; ++i) {
+            f.put(" w", 2);
+            f.put_int(c->word_label ? c->word_label[words[i]] : words[i]);
+        }
+        f.put('\n');
     }
     return f.close() ? CULDA_OK : CULDA_ERR_IO;
 }

@@ -3,6 +3,9 @@
 #include <stdarg.h>
 #include <stdint.h>
 
+#include <string>
+#include <vector>
+
 #include "../../include/culda_b200.h"
 
 namespace culda {
@@ -10,6 +13,9 @@ namespace culda {
 // Thread-local message of the last failed call that has no context.
 void set_global_error(const char *fmt, ...);
 const char *global_error();
+
+// Whole file into `buf`; false when it cannot be opened or read.
+bool read_file_bytes(const std::string &path, std::vector<char> &buf);
 
 // Host checks of a corpus descriptor (prefix arrays, doc ids, doc lengths).
 int validate_corpus(const culda_corpus *c);

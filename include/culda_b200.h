@@ -135,6 +135,36 @@ int culda_corpus_write_text(const culda_corpus *c, const char *path);
 
 void culda_corpus_free(culda_corpus *c);
 
+/* Token strings of a corpus read from text: word w's bytes are
+ * bytes[offsets[w] .. offsets[w+1]) (no terminator; any byte but whitespace). */
+typedef struct culda_vocab {
+    int32_t num_words;
+    int64_t *offsets;  /* [V+1] */
+    char *bytes;
+} culda_vocab;
+
+void culda_vocab_free(culda_vocab *v);
+
+/* Parse a text corpus (one document per line: a title field, then the
+ * document's whitespace-separated tokens; lines with no field are skipped) on
+ * `threads` host threads (0 = all), with word ids by first appearance.  This is
+ * the parsing half of the reference's preprocessing tool, src_format/format.cpp:56-90
+ * with src_culda/model/vocab.cpp:24-31.  `vocab` may be NULL.  Empty
+ * corpora and title-only documents are accepted, as the reference's tool accepts
+ * them. */
+int culda_corpus_from_text(const char *path, int32_t threads, culda_corpus **corpus, culda_vocab **vocab);
+
+/* Write the five src_format files for `c`, with the token strings of `vocab`
+ * in `.vocab` (NULL: "w<label>"), byte-identical to src_format/format.cpp:92-165
+ * and src_format/data_chunk.h:49-67, chunk-id suffixes when num_chunks > 1. */
+int culda_format_write(const culda_corpus *c, const culda_vocab *vocab, const char *prefix, int num_chunks);
+
+/* The reference's `format input output_prefix numChunks` tool
+ * (src_format/format.cpp:19-165) as one call: culda_corpus_from_text followed
+ * by culda_format_write.  An input that cannot be opened returns CULDA_ERR_IO
+ * with "<input> open failed" in culda_last_error(NULL). */
+int culda_format_text(const char *in_path, const char *out_prefix, int num_chunks, int32_t threads);
+
 /* doc_tok[N] (reference docRevIdx, doc_chunk.cpp:225-255) on the host. */
 int culda_corpus_doc_tokens(const culda_corpus *c, int32_t *doc_tok);
 

@@ -7,9 +7,10 @@
 // Extra options (off by default, so parsers of the reference's output keep
 // working): -seed <n> (Philox key, default 1), -G <lanes> (sampler lanes per
 // token), -j (print the FP64 joint log-likelihood on a separate line after
-// each iteration), -z <file> (write the final topics as int16).  -o <prefix>,
-// accepted and unused by the reference, writes <prefix>.topwords: each
-// topic's token count and its 20 most frequent words.
+// each iteration), -z <file> (write the final topics as int16), -top <n>
+// (words per topic in the -o report, default 20, 0 = all).  -o <prefix>,
+// accepted and unused by the reference, writes the topic-word and doc-topic
+// reports of the reference's commented-out saveWord / saveDoc.
 #include <algorithm>
 #include <cctype>
 #include <chrono>
@@ -29,7 +30,7 @@ struct Argument {  // src_culda/model/culda_argument.h:50-82
     float alpha = 0.f, beta = 0.f;
     std::string inputFilePrefix, outputFilePrefix, topicsOut;
     unsigned long long seed = 1;
-    int groupLanes = 0;
+    int groupLanes = 0, topWords = 20;
     bool jointLL = false;
 };
 
@@ -70,6 +71,7 @@ Argument parse(int argc, char **argv) {  // ParseArgument, main.cpp:40-161
         else if (o == "-G") a.groupLanes = integer("-G");
         else if (o == "-j") a.jointLL = true;
         else if (o == "-z") a.topicsOut = need("-z");
+        else if (o == "-top") a.topWords = atoi(need("-top"));
         else break;  // the reference stops at the first unknown token
     }
     // The reference leaves these uninitialised when absent; here they are required.
@@ -102,6 +104,116 @@ void print_argument(const Argument &a) {  // culda_argument.h:69-81
     printf("prefix      :%s\n", a.inputFilePrefix.c_str());
     printf("outfile     :%s\n", a.outputFilePrefix.c_str());
     printf("\n");
+}
+
+// Token strings from "<prefix>.vocab" ("token id" per line, src_format/format.cpp:96-99);
+// the word id as text for any word the file does not name.
+std::vector<std::string> load_vocab(const std::string &prefix, int V) {
+    std::vector<std::string> names((size_t)V);
+    for (int w = 0; w < V; ++w) names[(size_t)w] = std::to_string(w);
+    FILE *f = fopen((prefix + ".vocab").c_str(), "rb");
+    if (!f) return names;
+    std::string line;
+    int ch;
+    auto flush_line = [&]() {
+        const size_t sp = line.find_last_of(' ');
+        if (sp != std::string::npos && sp > 0 && sp + 1 < line.size()) {
+            const long id = strtol(line.c_str() + sp + 1, nullptr, 10);
+            if (id >= 0 && id < V) names[(size_t)id] = line.substr(0, sp);
+        }
+        line.clear();
+    };
+    while ((ch = fgetc(f)) != EOF) {
+        if (ch == '\n')
+            flush_line();
+        else
+            line.push_back((char)ch);
+    }
+    if (!line.empty()) flush_line();
+    fclose(f);
+    return names;
+}
+
+// -o <prefix>: the two model reports of the reference's commented-out
+// ModelPhi::saveWord (model_phi.cpp:283-329) and ModelTheta::saveDoc
+// (model_theta.cpp:207-242), in their layouts:
+//   <prefix>.topwords   "topic, total, top words", then per topic with tokens
+//                       "%4d total (token,count) ..." by count (ties: lower id
+//                       first), the first -top n words (0: all)
+//   <prefix>.doctopics  "Doc, total, top topics", then per doc
+//                       "%4d| total (topic,count), ..." over all its topics
+int write_reports(culda_ctx *ctx, const culda_corpus *corpus, const Argument &arg) {
+    const int K = arg.k, V = corpus->num_words, D = corpus->num_docs;
+    const int64_t N = corpus->num_tokens;
+    std::vector<int32_t> phi((size_t)V * K), nk((size_t)K);
+    std::vector<uint16_t> z((size_t)N);
+    int rc = culda_get_phi(ctx, phi.data(), nk.data());
+    if (rc == CULDA_OK) rc = culda_get_topics(ctx, z.data());
+    if (rc != CULDA_OK) {
+        fprintf(stderr, "Error: %s\n", culda_last_error(ctx));
+        return rc;
+    }
+    const std::vector<std::string> names = load_vocab(arg.inputFilePrefix, V);
+    std::string path = arg.outputFilePrefix + ".topwords";
+    FILE *f = fopen(path.c_str(), "w");
+    if (!f) {
+        fprintf(stderr, "Error: writing %s failed\n", path.c_str());
+        return CULDA_ERR_IO;
+    }
+    fprintf(f, "topic, total, top words\n");
+    std::vector<int32_t> idx;
+    for (int k = 0; k < K; ++k) {
+        idx.clear();
+        int64_t total = 0;
+        for (int w = 0; w < V; ++w)
+            if (phi[(size_t)w * K + k] > 0) {
+                idx.push_back(w);
+                total += phi[(size_t)w * K + k];
+            }
+        if (total <= 0) continue;
+        const size_t top = arg.topWords > 0 ? std::min(idx.size(), (size_t)arg.topWords) : idx.size();
+        std::partial_sort(idx.begin(), idx.begin() + (long)top, idx.end(), [&](int32_t a, int32_t b) {
+            const int32_t ca = phi[(size_t)a * K + k], cb = phi[(size_t)b * K + k];
+            return ca != cb ? ca > cb : a < b;
+        });
+        fprintf(f, "%4d %lld ", k, (long long)total);
+        for (size_t i = 0; i < top; ++i)
+            fprintf(f, "(%s,%d) ", names[(size_t)idx[i]].c_str(), phi[(size_t)idx[i] * K + k]);
+        fprintf(f, "\n");
+    }
+    if (fclose(f) != 0) return CULDA_ERR_IO;
+
+    std::vector<int32_t> doc_tok((size_t)N);
+    rc = culda_corpus_doc_tokens(corpus, doc_tok.data());
+    if (rc != CULDA_OK) return rc;
+    path = arg.outputFilePrefix + ".doctopics";
+    f = fopen(path.c_str(), "w");
+    if (!f) {
+        fprintf(stderr, "Error: writing %s failed\n", path.c_str());
+        return CULDA_ERR_IO;
+    }
+    fprintf(f, "Doc, total, top topics\n");
+    std::vector<uint16_t> topics;
+    std::vector<std::pair<int, int>> freq;  // (topic, count)
+    for (int d = 0; d < D; ++d) {
+        topics.clear();
+        for (int64_t i = corpus->doc_ptr[d]; i < corpus->doc_ptr[d + 1]; ++i) topics.push_back(z[(size_t)doc_tok[(size_t)i]]);
+        std::sort(topics.begin(), topics.end());
+        freq.clear();
+        for (size_t i = 0; i < topics.size();) {
+            size_t j = i;
+            while (j < topics.size() && topics[j] == topics[i]) ++j;
+            freq.emplace_back(topics[i], (int)(j - i));
+            i = j;
+        }
+        std::stable_sort(freq.begin(), freq.end(), [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+            return a.second > b.second;
+        });
+        fprintf(f, "%4d| %lld ", d, (long long)topics.size());
+        for (const auto &fr : freq) fprintf(f, "(%d,%d), ", fr.first, fr.second);
+        fprintf(f, "\n");
+    }
+    return fclose(f) == 0 ? CULDA_OK : CULDA_ERR_IO;
 }
 
 }  // namespace
@@ -171,35 +283,7 @@ int main(int argc, char **argv) {
         }
         if (f) fclose(f);
     }
-    // -o: the model summary the reference's commented-out saveWord
-    // (model_phi.cpp:283-329) would have written: per topic its token count
-    // and its 20 most frequent words (word id:count)
-    if (rc == CULDA_OK && !arg.outputFilePrefix.empty()) {
-        const int K = arg.k, V = corpus->num_words;
-        std::vector<int32_t> phi((size_t)V * K), nk((size_t)K);
-        rc = culda_get_phi(ctx, phi.data(), nk.data());
-        const std::string path = arg.outputFilePrefix + ".topwords";
-        FILE *f = rc == CULDA_OK ? fopen(path.c_str(), "w") : nullptr;
-        if (!f) {
-            fprintf(stderr, "Error: writing %s failed\n", path.c_str());
-            rc = CULDA_ERR_IO;
-        } else {
-            std::vector<int32_t> idx((size_t)V);
-            for (int k = 0; k < K; ++k) {
-                for (int w = 0; w < V; ++w) idx[(size_t)w] = w;
-                const int top = std::min(20, V);
-                std::partial_sort(idx.begin(), idx.begin() + top, idx.end(), [&](int32_t a, int32_t b) {
-                    const int32_t ca = phi[(size_t)a * K + k], cb = phi[(size_t)b * K + k];
-                    return ca != cb ? ca > cb : a < b;
-                });
-                fprintf(f, "topic %d tokens %d:", k, nk[(size_t)k]);
-                for (int i = 0; i < top && phi[(size_t)idx[(size_t)i] * K + k] > 0; ++i)
-                    fprintf(f, " %d:%d", idx[(size_t)i], phi[(size_t)idx[(size_t)i] * K + k]);
-                fprintf(f, "\n");
-            }
-            fclose(f);
-        }
-    }
+    if (rc == CULDA_OK && !arg.outputFilePrefix.empty()) rc = write_reports(ctx, corpus, arg);
     printf("\n");
     culda_destroy(ctx);
     culda_corpus_free(corpus);

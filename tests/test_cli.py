@@ -2,7 +2,9 @@
 its per-iteration output line (src_culda/main.cpp:40-194,
 src_culda/train/SingleChunkSingleGPU.h:127).  Argument and file errors are
 checked on the CPU; a short run on the GPU prints exactly the reference's line
-format and leaves the same topics as the library's own chain."""
+format, leaves the same topics as the library's own chain and writes the -o
+reports in the layouts of the reference's commented-out saveWord / saveDoc
+(src_culda/model/model_phi.cpp:283-329, model_theta.cpp:207-242)."""
 from __future__ import annotations
 
 import re
@@ -59,11 +61,26 @@ def test_run_prints_the_reference_line_and_matches_the_library(tmp_path):
         phi, nk = m.phi()
     printed = [float(LINE.match(ln).group(2)) for ln in lines]
     assert np.allclose(printed, lls, atol=1e-8)
+    vocab = dict(ln.rsplit(" ", 1)[::-1] for ln in (tmp_path / "c.vocab").read_text().splitlines())
     top = (tmp_path / "model.topwords").read_text().splitlines()
-    assert len(top) == 64
-    for k, ln in enumerate(top):
-        head, _, rest = ln.partition(":")
-        assert head == f"topic {k} tokens {nk[k]}"
-        pairs = [tuple(map(int, x.split(":"))) for x in rest.split()]
+    assert top[0] == "topic, total, top words"
+    rows = {}
+    for ln in top[1:]:
+        m = re.match(r"^ *(\d+) (\d+) ((?:\([^,()]+,\d+\) )*)$", ln)
+        assert m, ln
+        rows[int(m.group(1))] = (int(m.group(2)), re.findall(r"\(([^,()]+),(\d+)\)", m.group(3)))
+    assert sorted(rows) == [k for k in range(64) if nk[k] > 0]
+    for k, (total, pairs) in rows.items():
+        assert total == nk[k]
         want = sorted(((-phi[w, k], w) for w in range(phi.shape[0]) if phi[w, k] > 0))[:20]
-        assert pairs == [(w, -c) for c, w in want]
+        assert pairs == [(vocab[str(w)], str(-c)) for c, w in want]
+    doc = (tmp_path / "model.doctopics").read_text().splitlines()
+    assert doc[0] == "Doc, total, top topics" and len(doc) == c.num_docs + 1
+    doc_of = c.doc_ids  # doc of every token, word-major like the topics
+    for d, ln in enumerate(doc[1:]):
+        m = re.match(r"^ *(\d+)\| (\d+) ((?:\(\d+,\d+\), )*)$", ln)
+        assert m and int(m.group(1)) == d, ln
+        pairs = [(int(a), int(b)) for a, b in re.findall(r"\((\d+),(\d+)\)", m.group(3))]
+        ks, cs = np.unique(z_cli[doc_of == d], return_counts=True)
+        assert int(m.group(2)) == cs.sum()
+        assert pairs == sorted(zip(ks.tolist(), cs.tolist()), key=lambda kc: (-kc[1], kc[0]))

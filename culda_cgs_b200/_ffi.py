@@ -27,6 +27,7 @@ CULDA_ERR_NO_DEVICE = -8
 CULDA_LEN_POISSON, CULDA_LEN_LOGNORMAL, CULDA_LEN_PARETO = 0, 1, 2
 CULDA_NOALLOC_SCRATCH_BYTES = 8 << 20  # include/culda_b200.h
 CULDA_FLAG_NO_GRAPH, CULDA_FLAG_VERBOSE, CULDA_FLAG_NO_REORDER, CULDA_FLAG_AUTOTUNE = 1, 2, 4, 8
+CULDA_SAMPLER_FLAT = -1
 
 
 class Corpus(C.Structure):

@@ -5,8 +5,9 @@
 //   culda -g 1 -c 1 -k <topics> -t <iterations> -a <alpha> -b <beta> -i <prefix> [-o <prefix>] [-s n]
 //
 // Extra options (off by default, so parsers of the reference's output keep
-// working): -seed <n> (Philox key, default 1), -G <lanes> (sampler lanes per
-// token), -j (print the FP64 joint log-likelihood on a separate line after
+// working): -seed <n> (Philox key, default 1), -G <lanes> (a group sampler
+// with that many lanes per token instead of the default warp-flattened walk),
+// -j (print the FP64 joint log-likelihood on a separate line after
 // each iteration), -z <file> (write the final topics as int16), -top <n>
 // (words per topic in the -o report, default 20, 0 = all).  -o <prefix>,
 // accepted and unused by the reference, writes the topic-word and doc-topic

@@ -216,8 +216,10 @@ constexpr uint32_t kTuneIteration = 3;
 // uniforms once, then per variant one warm-up and two timed launches that
 // write the other topic buffer.  The context's state does not change.
 int autotune_sampler(culda_ctx *ctx) {
-    static const int kCands[][2] = {{4, kSampleBlocksHigh}, {8, kSampleBlocksHigh}, {16, kSampleBlocksHigh},
-                                    {2, kSampleBlocksDefault}, {4, kSampleBlocksDefault}, {8, kSampleBlocksDefault}};
+    static const int kCands[][2] = {{kFlatLanes, kSampleBlocksDefault}, {4, kSampleBlocksHigh},
+                                    {8, kSampleBlocksHigh},                {16, kSampleBlocksHigh},
+                                    {2, kSampleBlocksDefault},             {4, kSampleBlocksDefault},
+                                    {8, kSampleBlocksDefault}};
     const std::string key = tune_key(ctx);
     TuneResult best;
     if (tune_lookup(key, best)) {
@@ -267,7 +269,7 @@ int autotune_sampler(culda_ctx *ctx) {
     int32_t e = 0;
     CK(cudaMemcpy(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost));
     if (e) return fail(ctx, CULDA_ERR_DEVICE_STATE, "autotune: sampler reported device error 0x%x", e);
-    if (best.group_lanes == 0) return fail(ctx, CULDA_ERR_CUDA, "autotune: no sampler variant fits the device");
+    if (best.ms == 0.f) return fail(ctx, CULDA_ERR_CUDA, "autotune: no sampler variant fits the device");
     ctx->group_lanes = best.group_lanes;
     ctx->sample_blocks = best.sample_blocks;
     ctx->sample_grid = std::max(
@@ -307,11 +309,13 @@ int build_graphs(culda_ctx *ctx) {
 namespace {
 
 int pick_group_lanes(int requested, int k) {
-    if (requested == 1 || requested == 2 || requested == 4 || requested == 8 || requested == 16 || requested == 32)
+    if (requested == kFlatLanes || requested == 1 || requested == 2 || requested == 4 || requested == 8 ||
+        requested == 16 || requested == 32)
         return requested;
-    // measured on the 60M-token workload (K = 1024): 4 lanes per token with the
-    // 64-register budget is the fastest variant
-    return requested == 0 ? (k <= 2048 ? 4 : 8) : -1;
+    // the warp-flattened walk is the fastest variant on every measured
+    // workload (60M tokens at K = 1024; 118M uneven tokens at K = 256..4096)
+    (void)k;
+    return requested == 0 ? kFlatLanes : 0;  // 0: not a variant
 }
 
 int pick_sample_blocks(int requested) { return requested != 0 ? requested : kSampleBlocksDefault; }
@@ -537,7 +541,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     if ((p->flags & CULDA_FLAG_AUTOTUNE) && (p->group_lanes != 0 || p->sample_blocks != 0))
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: CULDA_FLAG_AUTOTUNE needs group_lanes = sample_blocks = 0");
     const int gl = pick_group_lanes(p->group_lanes, p->k);
-    if (gl < 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: group_lanes=%d", p->group_lanes);
+    if (gl == 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: group_lanes=%d", p->group_lanes);
     const int sb = pick_sample_blocks(p->sample_blocks);
     if (!sample_variant_exists(gl, sb))
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: no sampler for group_lanes=%d sample_blocks=%d", gl,

@@ -493,8 +493,8 @@ extern "C" int culda_sample(const culda_sample_args *a, void *d_workspace, size_
         !a->loglik_sum || !d_workspace ||
         (a->num_hot > 0 && (!a->hot_items || a->num_hot_items <= 0)) || a->theta_capacity <= 0 ||
         workspace_bytes < culda_sample_workspace(a->k, a->num_items, a->num_hot) ||
-        (a->group_lanes != 1 && a->group_lanes != 2 && a->group_lanes != 4 && a->group_lanes != 8 &&
-         a->group_lanes != 16 && a->group_lanes != 32) ||
+        (a->group_lanes != kFlatLanes && a->group_lanes != 1 && a->group_lanes != 2 && a->group_lanes != 4 &&
+         a->group_lanes != 8 && a->group_lanes != 16 && a->group_lanes != 32) ||
         ((uintptr_t)a->theta & 15u)) {
         set_global_error("culda_sample: invalid argument");
         return CULDA_ERR_INVALID_ARG;

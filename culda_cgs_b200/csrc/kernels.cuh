@@ -65,12 +65,14 @@ inline int pow2_ceil(int k) {
     return p;
 }
 
-size_t sample_smem_bytes(int k);
 // Sampler variants: lanes per token G and the register budget, given as the
 // resident CTAs per SM the kernel is compiled for (kSampleBlocksDefault for
-// every G; kSampleBlocksHigh for G = 4, 8, 16).
+// every G; kSampleBlocksHigh for G = 4, 8, 16).  G = kFlatLanes is the
+// warp-flattened walk (kSampleBlocksDefault only).
 constexpr int kSampleBlocksDefault = 8;
 constexpr int kSampleBlocksHigh = 10;
+constexpr int kFlatLanes = -1;
+size_t sample_smem_bytes(int k, int group_lanes);
 bool sample_variant_exists(int group_lanes, int blocks_per_sm);
 int sample_blocks_per_sm(int k, int group_lanes, int blocks_per_sm);
 cudaError_t launch_sample(const SampleParams &p, int group_lanes, int blocks_per_sm, int grid, cudaStream_t s);

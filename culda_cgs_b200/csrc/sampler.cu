@@ -426,7 +426,371 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_kernel(const Samp
     }
 }
 
-size_t sample_smem_bytes(int k) {
+// ------------------------------------------------------ the flat walk
+// The warp-flattened sampler (group_lanes = kFlatLanes, -1).  A warp takes up to
+// 32 consecutive segments of the item and splits the 8-entry units of their
+// rows into 8 contiguous ranges of 4r units (r odd), one per group of 4
+// lanes.  Rows start and end on multiples of 32 entries, i.e. of 4 units, so
+// a group step (4 units, one 128-byte line) never straddles two rows.  Each
+// group walks its range once with a compensated running sum that restarts at
+// every row start and stores every unit's running prefix; a segmented scan
+// over the groups' last values gives each group the sum carried into its
+// range, which completes the prefixes of the units before its first row
+// start.  With every unit's inclusive prefix inside its row in shared memory,
+// each lane draws its own tokens: a binary search for the first unit whose
+// prefix exceeds the target and a sequential pass over that unit's 8 entries.
+// All groups stay busy whatever the mix of row lengths, and no lane waits on
+// another token's draw.
+constexpr int kUnit = kLaneEntries;               // entries per unit: two 16-byte loads
+constexpr int kFlatWarps = kSampleThreads / 32;
+constexpr int kFlatSegs = 32;                     // segments a warp takes at a time
+constexpr int kFlatMeta = 2 * (kFlatSegs + 1) + 4 * kFlatSegs;  // ints of per-warp segment data
+constexpr int kWalkLanes = 4;                     // lanes walking one range: 4 units, 128 bytes, per step
+
+// Units of one warp batch: at least a whole row of K entries (K / 8 units).
+__host__ __device__ constexpr int flat_unit_budget(int k) { return k / kUnit > 256 ? k / kUnit : 256; }
+
+__device__ __forceinline__ Step load_unit(const ThetaEntry *__restrict__ theta, int idx) {
+    Step st;
+#pragma unroll
+    for (int j = 0; j < kLaneVecs; ++j) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(theta + idx) + j);
+        st.e[4 * j] = v.x;
+        st.e[4 * j + 1] = v.y;
+        st.e[4 * j + 2] = v.z;
+        st.e[4 * j + 3] = v.w;
+    }
+    return st;
+}
+
+// Largest i in [0, n) with a[i] <= x, for non-decreasing a with a[0] <= x.
+__device__ __forceinline__ int last_le(const int *a, int n, int x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// The first entry of a unit whose running sum, from `prev`, exceeds T; the
+// unit's last non-zero entry when rounding leaves the unit short of T (-1 for
+// a unit without non-zero entries).
+__device__ __forceinline__ int resolve_unit(const Step &st, float prev, float T, const float *ph) {
+    float part = 0.f;
+    int hit = -1, last = -1;
+#pragma unroll
+    for (int j = 0; j < kUnit; ++j) {
+        part = fsum(part, entry_prob(st.e[j], ph));
+        const bool nz = entry_count(st.e[j]) != 0u;
+        if (nz) last = entry_topic(st.e[j]);
+        if (hit < 0 && nz && fsum(prev, part) > T) hit = entry_topic(st.e[j]);
+    }
+    return hit >= 0 ? hit : last;
+}
+
+// The row's last non-zero entry: rows hold their non-zero entries first and
+// zero padding after them, up to the next multiple of 32, so it lies in the
+// final 32-entry block.
+__device__ __forceinline__ int row_last_nonzero(const ThetaEntry *__restrict__ theta, int rs, int re) {
+    int last = -1;
+    for (int i = max(rs, re - 32); i < re; ++i) {
+        const ThetaEntry e = __ldg(theta + i);
+        if (entry_count(e)) last = entry_topic(e);
+    }
+    return last;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const SampleParams p) {
+    extern __shared__ float smem[];
+    const int K = p.k, KP = p.kmask + 1, B = flat_unit_budget(K);
+    float *ph = smem;               // [KP] phihat of the current word (zero past K), at offset 0
+    float *inv = smem + KP;         // [K]  1 / (n_k + V beta)
+    float *qc = inv + K;            // [K]  dense-bucket prefix (the word histogram before that)
+    int *hist = reinterpret_cast<int *>(qc);
+    __shared__ int s_item, s_chunk;
+    __shared__ float s_warp[kSampleThreads / 32];
+    __shared__ double s_red[kSampleThreads / 32];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wl = lane & (kWalkLanes - 1), wg = lane / kWalkLanes;  // lane in its walk group, group
+    const unsigned wm = group_mask<kWalkLanes>(lane);
+    float *ub = qc + K + warp * B;  // [B] unit prefixes of the warp's batch
+    int *m_cum = reinterpret_cast<int *>(qc + K + kFlatWarps * B) + warp * kFlatMeta;
+    int *m_tc = m_cum + (kFlatSegs + 1);  // [n+1] first unit / first token (flat) of each segment
+    int *m_rs = m_tc + (kFlatSegs + 1);   // [n] row start (entry index)
+    int *m_t0 = m_rs + kFlatSegs;         // [n] first token
+    float *m_S = reinterpret_cast<float *>(m_t0 + kFlatSegs);  // [n] S of the row
+    float *m_lg = m_S + kFlatSegs;                               // [n] log(S + Q)
+    const uint32_t iter = p.iteration_ptr ? *p.iteration_ptr : p.iteration;
+
+    for (int j = tid; j < K; j += blockDim.x) inv[j] = 1.0f / ((float)p.nk[j] + p.vbeta);
+    for (int j = K + tid; j < KP; j += blockDim.x) ph[j] = 0.f;
+
+    for (;;) {
+        if (tid == 0) {
+            s_item = atomicAdd(p.item_counter, 1);
+            s_chunk = 0;
+        }
+        __syncthreads();
+        const int it = s_item;
+        if (it >= p.num_items) break;
+        const culda_item item = p.items[it];
+        const int64_t ibeg = item.begin, iend = item.begin + item.count;
+        if (ibeg < 0 || item.count < 0 || iend > p.num_tokens || item.hot >= p.num_hot || item.seg_begin < 0 ||
+            item.seg_count < 0 || (int64_t)item.seg_begin + item.seg_count > p.num_segs) {
+            if (tid == 0) {
+                atomicOr(p.error, kErrRowRange);
+                p.item_ll[it] = 0.0;
+            }
+            __syncthreads();  // s_item is rewritten only after every thread has read it
+            continue;
+        }
+
+        // phi row of the word
+        const int *src;
+        if (p.frozen_phi) {
+            src = p.frozen_phi + (size_t)item.word * K;
+        } else if (item.hot < 0) {
+            for (int j = tid; j < K; j += blockDim.x) hist[j] = 0;
+            __syncthreads();
+            for (int64_t t = ibeg + tid; t < iend; t += blockDim.x) {
+                const uint32_t z = p.topics_in[t];
+                if (z < (uint32_t)K)
+                    atomicAdd(&hist[z], 1);
+                else
+                    atomicOr(p.error, kErrTopicRange);
+            }
+            __syncthreads();
+            src = hist;
+        } else {
+            src = p.hot_phi + (size_t)item.hot * K;
+        }
+        for (int j = tid; j < K; j += blockDim.x) ph[j] = ((float)src[j] + p.beta) * inv[j];
+        __syncthreads();
+        dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
+        __syncthreads();
+        const float Q = qc[K - 1];
+
+        double ll = 0.0;
+        const int sg_end = item.seg_begin + item.seg_count;
+        // chunks of a quarter of the item's segments (8 to 32), so the four
+        // warps share small items too
+        const int cs = min(kFlatSegs, max(8, (item.seg_count + kFlatWarps - 1) / kFlatWarps));
+        for (;;) {
+            int ch = 0;
+            if (lane == 0) ch = atomicAdd(&s_chunk, 1);
+            ch = __shfl_sync(0xffffffffu, ch, 0);
+            if ((int64_t)ch * cs >= item.seg_count) break;
+            const int seg0 = item.seg_begin + ch * cs;
+            const int nseg = min(cs, sg_end - seg0);
+
+            // lane s holds segment seg0 + s: its tokens, doc and theta row
+            int rs = 0, nu = 0, t0 = 0, tcount = 0;
+            if (lane < nseg) {
+                const int sg = seg0 + lane;
+                const int64_t a0 = __ldg(p.seg_start + sg);
+                const int64_t a1 = sg + 1 < sg_end ? (int64_t)__ldg(p.seg_start + sg + 1) : iend;
+                if (a0 < ibeg || a1 > iend || a0 >= a1) {
+                    atomicOr(p.error, kErrRowRange);
+                } else {
+                    const int d = __ldg(p.doc_ids + a0);
+                    if ((unsigned)d < (unsigned)p.num_docs) {
+                        const int2 r = __ldg(p.rows + d);
+                        if (r.x >= 0 && r.x <= r.y && (int64_t)r.y <= p.theta_cap && ((r.x | r.y) & 31) == 0 &&
+                            r.y - r.x <= kUnit * B) {
+                            rs = r.x;
+                            nu = (r.y - r.x) / kUnit;
+                            t0 = (int)a0;
+                            tcount = (int)(a1 - a0);
+                        } else {
+                            atomicOr(p.error, kErrRowRange);
+                        }
+                    } else {
+                        atomicOr(p.error, kErrDocRange);
+                    }
+                }
+            }
+
+            int done = 0;
+            while (done < nseg) {
+                // the batch: segments [done, last] whose units fit the budget
+                const bool act = lane >= done && lane < nseg;
+                const int v = act ? nu : 0;
+                const int incl = warp_incl_scan(v, lane);
+                const unsigned fm = __ballot_sync(0xffffffffu, act && incl <= B);
+                const int last = 31 - __clz(fm);  // lane `done` always fits: nu <= B
+                const int n = last - done + 1;
+                const bool mine = act && lane <= last;
+                const int tc = mine ? tcount : 0;
+                const int tincl = warp_incl_scan(tc, lane);
+                const int total_u = __shfl_sync(0xffffffffu, incl, last);
+                const int total_t = __shfl_sync(0xffffffffu, tincl, last);
+                if (mine) {
+                    const int i = lane - done;
+                    m_cum[i] = incl - v;
+                    m_tc[i] = tincl - tc;
+                    m_rs[i] = rs;
+                    m_t0[i] = t0;
+                    if (lane == last) {
+                        m_cum[n] = incl;
+                        m_tc[n] = tincl;
+                    }
+                }
+                __syncwarp();
+
+                // walk: group g (lanes 4g..4g+3) takes units [gb, ge), 4 per step,
+                // a step being one 128-byte line of one row; the running sum
+                // restarts at every row start
+                const int r = ((total_u + 31) >> 5) | 1;  // odd: the 8 groups' stores hit distinct banks
+                const int gb = min(wg * 4 * r, total_u), ge = min(gb + 4 * r, total_u);
+                float gv = 0.f;
+                int gflag = 0, lead_end = gb;
+                if (gb < ge) {
+                    int sp = last_le(m_cum, n, gb);
+                    int nxt = m_cum[sp + 1], rowu = m_cum[sp], rbase = m_rs[sp];
+                    gflag = gb == rowu;
+                    lead_end = gflag ? gb : min(nxt, ge);
+                    float s = 0.f, c = 0.f;
+                    Step cur = load_unit(p.theta, rbase + kUnit * (gb + wl - rowu));
+                    for (int u0 = gb;;) {
+                        const int u1 = u0 + kWalkLanes;
+                        bool reset1 = false;
+                        if (u1 < ge && u1 == nxt) {
+                            do {
+                                ++sp;
+                                nxt = m_cum[sp + 1];
+                            } while (nxt == u1);
+                            rowu = u1;
+                            rbase = m_rs[sp];
+                            reset1 = true;
+                        }
+                        Step nx;
+                        if (u1 < ge) nx = load_unit(p.theta, rbase + kUnit * (u1 + wl - rowu));
+                        float pr[kUnit];
+                        step_probs(cur, ph, pr);
+                        float incl = lane_sum(pr);
+#pragma unroll
+                        for (int o = 1; o < kWalkLanes; o <<= 1) {
+                            const float t = __shfl_up_sync(wm, incl, o, kWalkLanes);
+                            if (wl >= o) incl = fsum(incl, t);
+                        }
+                        const float tot = __shfl_sync(wm, incl, kWalkLanes - 1, kWalkLanes);
+                        ub[u0 + wl] = fsum(s + c, incl);
+                        neumaier(s, c, tot);
+                        if (u1 >= ge) break;
+                        if (reset1) {
+                            s = 0.f;
+                            c = 0.f;
+                            gflag = 1;
+                        }
+                        u0 = u1;
+                        cur = nx;
+                    }
+                    gv = s + c;
+                }
+                // segmented scan over the groups: the running row sum entering each range
+                double vd = (double)gv;
+                int fl = gflag;
+#pragma unroll
+                for (int o = kWalkLanes; o < 32; o <<= 1) {
+                    const double vo = __shfl_up_sync(0xffffffffu, vd, o);
+                    const int fo = __shfl_up_sync(0xffffffffu, fl, o);
+                    if (lane >= o && !fl) {
+                        vd += vo;
+                        fl = fo;
+                    }
+                }
+                double carry = __shfl_up_sync(0xffffffffu, vd, kWalkLanes);
+                if (lane < kWalkLanes) carry = 0.0;
+                if (gb < lead_end) {
+                    const float cf = (float)carry;
+                    for (int u = gb + wl; u < lead_end; u += kWalkLanes) ub[u] = fsum(ub[u], cf);
+                }
+                __syncwarp();
+                if (mine) {
+                    const int i = lane - done;
+                    const int c0 = m_cum[i], c1 = m_cum[i + 1];
+                    const float S = c1 > c0 ? ub[c1 - 1] : 0.f;
+                    m_S[i] = S;
+                    m_lg[i] = logf(S + Q);
+                }
+                __syncwarp();
+
+                // draws: lane f takes the batch's tokens f, f + 32, ...
+                for (int f = lane; f < total_t; f += 32) {
+                    const int i = last_le(m_tc, n, f);
+                    const int tok = m_t0[i] + (f - m_tc[i]);
+                    float um;
+                    if (p.uniforms) {
+                        um = __ldg(p.uniforms + tok);
+                    } else {
+                        const int64_t key = p.tok_index ? (int64_t)__ldg(p.tok_index + tok) : (int64_t)tok;
+                        um = uniform_from_bits(philox_token(p.seed, (uint64_t)key, iter, kPurposeSample));
+                    }
+                    const float S = m_S[i];
+                    const float T = um * (S + Q);
+                    int z;
+                    if (T < S) {
+                        const int c0 = m_cum[i];
+                        int lo = c0, hi = m_cum[i + 1] - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (ub[mid] > T)
+                                hi = mid;
+                            else
+                                lo = mid + 1;
+                        }
+                        const float prev = lo > c0 ? ub[lo - 1] : 0.f;
+                        z = resolve_unit(load_unit(p.theta, m_rs[i] + kUnit * (lo - c0)), prev, T, ph);
+                        // a unit of the row's padding: T lies within a rounding of the
+                        // prefix where that unit starts (a lane's carried-in sum can round
+                        // one unit in the last place above the previous unit's prefix)
+                        if (z < 0) z = row_last_nonzero(p.theta, m_rs[i], m_rs[i] + kUnit * (m_cum[i + 1] - c0));
+                    } else {
+                        z = dense_bucket_search<1>(qc, K, T - S, 0, 0u, lane);
+                    }
+                    if (z < 0) {
+                        atomicOr(p.error, kErrRowRange);
+                        z = 0;
+                    }
+                    p.topics_out[tok] = (uint16_t)z;
+                    ll += (double)m_lg[i];
+                }
+                __syncwarp();  // the batch's shared data is read before the next batch writes it
+                done = last + 1;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ll += __shfl_down_sync(0xffffffffu, ll, o);
+        if (lane == 0) s_red[warp] = ll;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kSampleThreads / 32; ++w) s += s_red[w];
+            p.item_ll[it] = s;
+        }
+    }
+}
+
+size_t sample_smem_bytes(int k, int group_lanes) {
+    if (group_lanes == kFlatLanes)  // ph[pow2(K)] + inv[K] + qc[K] + per warp: unit prefixes and segment data
+        return ((size_t)2 * k + (size_t)pow2_ceil(k) + (size_t)kFlatWarps * flat_unit_budget(k) +
+                (size_t)kFlatWarps * kFlatMeta) *
+               sizeof(float);
     // ph[pow2(K)] + inv[K] + qc[K] + the per-group running sums
     return ((size_t)2 * k + (size_t)pow2_ceil(k) + (size_t)SampleShape<1>::kPrefixFloats) * sizeof(float);
 }
@@ -437,6 +801,9 @@ static const void *sample_fn() {
 }
 
 static const void *sample_kernel_for(int g, int minb) {
+    if (g == kFlatLanes)
+        return minb == kSampleBlocksDefault ? reinterpret_cast<const void *>(&sample_flat_kernel<kSampleBlocksDefault>)
+                                            : nullptr;
     if (minb == kSampleBlocksDefault) switch (g) {
             case 1: return sample_fn<1, kSampleBlocksDefault>();
             case 2: return sample_fn<2, kSampleBlocksDefault>();
@@ -462,7 +829,7 @@ bool sample_variant_exists(int group_lanes, int blocks_per_sm) {
 int sample_blocks_per_sm(int k, int group_lanes, int blocks_per_sm) {
     const void *fn = sample_kernel_for(group_lanes, blocks_per_sm);
     if (!fn) return 0;
-    const size_t smem = sample_smem_bytes(k);
+    const size_t smem = sample_smem_bytes(k, group_lanes);
     if (allow_smem(fn, smem, nullptr) != cudaSuccess) return 0;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kSampleThreads, smem) != cudaSuccess) return 0;
@@ -470,7 +837,7 @@ int sample_blocks_per_sm(int k, int group_lanes, int blocks_per_sm) {
 }
 
 cudaError_t launch_sample(const SampleParams &p, int group_lanes, int blocks_per_sm, int grid, cudaStream_t s) {
-    const size_t smem = sample_smem_bytes(p.k);
+    const size_t smem = sample_smem_bytes(p.k, group_lanes);
     void *args[] = {const_cast<SampleParams *>(&p)};
     const void *fn = sample_kernel_for(group_lanes, blocks_per_sm);
     if (!fn) return cudaErrorInvalidValue;

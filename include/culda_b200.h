@@ -175,12 +175,18 @@ typedef struct culda_params {
     float beta;           /* reference: -b */
     uint64_t seed;        /* Philox key for init and sampling */
     int32_t device;       /* CUDA device ordinal */
-    int32_t group_lanes;  /* lanes per token in the sampler: 0 = auto, else 1,2,4,8,16,32 */
+    int32_t group_lanes;  /* sampler variant: 0 = auto, CULDA_SAMPLER_FLAT (-1) = the warp-flattened
+                             walk, else 1,2,4,8,16,32 lanes per token */
     int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto, at most 65535 */
     int32_t flags;        /* CULDA_FLAG_* */
     int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (8),
                               8 (<= 64 registers), or 10 (<= 48 registers; group_lanes 4, 8, 16) */
 } culda_params;
+
+/* group_lanes value of the warp-flattened sampler: a warp splits the rows of up
+ * to 32 segments evenly over its lanes, builds every row's prefix sums in shared
+ * memory, and each lane then draws its own tokens. */
+enum { CULDA_SAMPLER_FLAT = -1 };
 
 enum {
     CULDA_FLAG_NO_GRAPH = 1,      /* launch the iteration kernel by kernel instead of one CUDA graph */
@@ -365,7 +371,7 @@ typedef struct culda_sample_args {
     int64_t theta_capacity;      /* entries in theta (rows are checked against it) */
     uint64_t seed;
     uint32_t iteration;          /* Philox counter word 2 */
-    int32_t group_lanes;         /* 1,2,4,8,16,32 */
+    int32_t group_lanes;         /* CULDA_SAMPLER_FLAT or 1,2,4,8,16,32 */
     double *loglik_sum;          /* device double: receives sum over tokens of log(S+Q) */
     int32_t *error;              /* device int32 error word (optional) */
 } culda_sample_args;

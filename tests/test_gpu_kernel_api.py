@@ -79,7 +79,7 @@ def test_update_theta(problem):
     assert int(host(p.d["ws_theta"], np.int32)[0]) == 0
 
 
-@pytest.mark.parametrize("g", [1, 8, 32])
+@pytest.mark.parametrize("g", [1, 8, 32, -1])
 def test_sample_and_loglik(problem, g):
     import torch
 

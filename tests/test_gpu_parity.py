@@ -68,6 +68,12 @@ CASES = [  # name, corpus, K, lanes per token, item tokens (0 = auto), sampler r
     ("mini-k1024-g4-b10-hot", MINI.gen, 1024, 4, 300, 10),
     ("mini-k1024-g16-b10", MINI.gen, 1024, 16, 0, 10),
     ("tiny-k64-g8-b10", TINY.gen, 64, 8, 0, 10),
+    ("tiny-k64-flat", TINY.gen, 64, -1, 0, 0),
+    ("tiny-k32-flat-hot", TINY.gen, 32, -1, 40, 0),
+    ("mini-k1024-flat", MINI.gen, 1024, -1, 0, 0),
+    ("mini-k1024-flat-hot", MINI.gen, 1024, -1, 300, 0),
+    ("mini-k256-flat", MINI.gen, 256, -1, 0, 0),
+    ("mini-k4096-flat", MINI.gen, 4096, -1, 0, 0),
 ]
 
 
@@ -108,7 +114,7 @@ def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens, 
         assert np.array_equal(m.topics(), s.z)
 
 
-@pytest.mark.parametrize("g,blocks", [(1, 8), (4, 8), (8, 8), (32, 8), (8, 10)])
+@pytest.mark.parametrize("g,blocks", [(1, 8), (4, 8), (8, 8), (32, 8), (8, 10), (-1, 8)])
 def test_long_chain_keeps_device_state_consistent(g, blocks):
     """~10M draws per sampler variant: tokens whose target lands within a rounding
     of a bucket boundary must still get a topic (the sampler's error word stays 0)."""
@@ -171,7 +177,7 @@ EDGE = {
 
 
 @pytest.mark.parametrize("name", list(EDGE))
-@pytest.mark.parametrize("g", [1, 8])
+@pytest.mark.parametrize("g", [1, 8, -1])
 def test_edge_corpora(name, g):
     c = _corpus(EDGE[name])
     k = 32

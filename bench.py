@@ -198,6 +198,12 @@ def ncu_traffic(workload: str):
         return None
 
 
+def run_flags(args) -> int:
+    import culda_cgs_b200 as cb
+
+    return (cb.CULDA_FLAG_AUTOTUNE if args.autotune else 0) | (cb.CULDA_FLAG_NO_REORDER if args.no_reorder else 0)
+
+
 def workload(args, seed: int):
     """The named workload with the run's seed; --k replaces K (and alpha = 50/K)."""
     from dataclasses import replace
@@ -333,7 +339,7 @@ def run_ours(args, world, rank, local, pg):
     # ---- device-resident measurement
     m = cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed + rank, device=local, group_lanes=args.group_lanes,
                item_tokens=args.item_tokens, sample_blocks=args.sample_blocks,
-               flags=cb.CULDA_FLAG_AUTOTUNE if args.autotune else 0)
+               flags=run_flags(args))
     info = m.info()
     log(f"[rank {rank}] info {info}")
     clocks = ClockSampler(local)
@@ -397,7 +403,7 @@ def run_ours(args, world, rank, local, pg):
         t0 = time.perf_counter()
         m2 = cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed + rank, device=local,
                     group_lanes=args.group_lanes, item_tokens=args.item_tokens, sample_blocks=args.sample_blocks,
-                    flags=cb.CULDA_FLAG_AUTOTUNE if args.autotune else 0)
+                    flags=run_flags(args))
         lls = [s["loglik"] for s in m2.iterate(args.steps)]
         st = cb.lib().culda_get_topics(m2._ctx, C.cast(z_host.data_ptr(), C.POINTER(C.c_uint16)))
         cuda_sync()
@@ -452,6 +458,7 @@ def run_ours(args, world, rank, local, pg):
         "config": {"workload": wl.name, "num_tokens": N, "num_docs": corpus.num_docs, "num_words": corpus.num_words,
                    "k": wl.k, "alpha": wl.alpha, "beta": wl.beta, "seed": args.seed,
                    "group_lanes": info["group_lanes"], "sample_blocks": info["sample_blocks"],
+                   "token_order": "input" if args.no_reorder else "by doc length inside each word",
                    "autotuned": bool(info["tuned"]),
                    "items": info["num_items"], "hot_words": info["num_hot"],
                    "l2": f"inputs larger than L2 (resident set {info['device_bytes'] / 1e9:.2f} GB > 126 MB)",
@@ -535,6 +542,7 @@ def main():
     ap.add_argument("--item-tokens", type=int, default=0)
     ap.add_argument("--sample-blocks", type=int, default=0, help="sampler register budget (CTAs per SM): 0, 8, 10")
     ap.add_argument("--autotune", action="store_true", help="time the sampler variants at create and keep the fastest")
+    ap.add_argument("--no-reorder", action="store_true", help="keep tokens in input order inside each word")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iterations", type=int, default=2)

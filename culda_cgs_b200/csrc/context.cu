@@ -451,6 +451,30 @@ __global__ void item_segments_kernel(culda_item *items, int num_items, const int
 // One device buffer for the set-up's temporaries (sort keys and values, scan
 // arrays, CUB scratch), carved by a bump allocator and released once: set-up
 // makes one allocation and one free instead of one pair per temporary.
+// A process-wide pool of pinned DevStats slots: a cudaMallocHost costs
+// milliseconds, so contexts take slots from shared pinned pages and give them
+// back on destroy (the pages live as long as the process).
+std::mutex g_pinned_mu;
+std::vector<DevStats *> g_pinned_free;
+
+DevStats *pinned_stats_get() {
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    if (g_pinned_free.empty()) {
+        constexpr int kSlots = 64;
+        DevStats *page = nullptr;
+        if (cudaMallocHost((void **)&page, sizeof(DevStats) * kSlots) != cudaSuccess) return nullptr;
+        for (int i = kSlots - 1; i >= 0; --i) g_pinned_free.push_back(page + i);
+    }
+    DevStats *p = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    return p;
+}
+
+void pinned_stats_put(DevStats *p) {
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free.push_back(p);
+}
+
 struct SetupArena {
     char *base = nullptr;
     size_t size = 0, used = 0;
@@ -514,8 +538,7 @@ int build_segments_device(culda_ctx *ctx, SetupArena &arena) {
         int32_t total = 0;
         CKS(cudaMemcpyAsync(&total, index + N, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         CKS(cudaStreamSynchronize(s));
-        ctx->num_segs = total;
-        CKS(dalloc(&ctx->d_seg_start, (size_t)total));
+        ctx->num_segs = total;  // d_seg_start holds one entry per token, the most there can be
         seg_scatter_kernel<<<grid(N), 256, 0, s>>>(N, flag, index, ctx->d_seg_start);
         item_segments_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, index);
         CKS(cudaGetLastError());
@@ -621,46 +644,148 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         t_last = now;
     };
 
+    // ---- host-side layout first: every persistent buffer's size is known
+    // before the device is touched, so they all come from one allocation
+    // (each cudaMalloc / cudaFree costs about a millisecond)
+    const bool reorder = !(p->flags & CULDA_FLAG_NO_REORDER);
+    // theta layout: capacity roundup32(min(L_d, K)) per doc (model_theta.cpp:50-56)
+    ctx->h_doc_ptr.assign(c->doc_ptr, c->doc_ptr + D + 1);
+    ctx->h_max_ia.resize((size_t)D + 1);
+    std::vector<int2> rows((size_t)D);
+    {
+        std::vector<int64_t> docs_of_len(65536, 0);  // doc lengths are below 65536 (checked above)
+        int64_t off = 0;
+        for (int32_t d = 0; d < D; ++d) {
+            int64_t len = c->doc_ptr[d + 1] - c->doc_ptr[d];
+            docs_of_len[(size_t)len]++;
+            if (len > K) len = K;
+            len = (len + 31) / 32 * 32;
+            if (off + len >= (int64_t)INT32_MAX) {
+                fail(ctx, CULDA_ERR_UNSUPPORTED, "culda_create: theta capacity exceeds int32 offsets");
+                return bail(CULDA_ERR_UNSUPPORTED);
+            }
+            ctx->h_max_ia[d] = (int32_t)off;
+            rows[d] = make_int2((int)off, (int)off);
+            off += len;
+        }
+        ctx->h_max_ia[D] = (int32_t)off;
+        ctx->theta_cap = off;
+        // sum_d L_d log(L_d + K alpha), one logarithm per distinct length
+        for (size_t len = 1; len < docs_of_len.size(); ++len)
+            if (docs_of_len[len])
+                ctx->doc_term +=
+                    (double)docs_of_len[len] * (double)len * std::log((double)len + (double)K * (double)p->alpha);
+    }
+    // docs longest first for the theta rebuild's warps: a counting sort on
+    // the length (below 65536), stable in doc id
+    std::vector<int32_t> doc_order((size_t)D);
+    {
+        std::vector<int32_t> start(65537, 0);
+        for (int32_t d = 0; d < D; ++d) start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d])) + 1]++;
+        for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+        for (int32_t d = 0; d < D; ++d)
+            doc_order[(size_t)start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d]))]++] = d;
+    }
+    // grids
+    const int sms = num_sms(ctx->device);
+    int sbps = sample_blocks_per_sm(K, gl, sb);
+    if (sbps <= 0) {
+        fail(ctx, CULDA_ERR_CUDA, "culda_create: sampler does not fit on the device for K=%d", K);
+        return bail(CULDA_ERR_CUDA);
+    }
+    int tbps = theta_blocks_per_sm(K);
+    if (tbps <= 0) tbps = 1;
+    ctx->theta_grid = std::max(1, std::min(sms * tbps, (D + kThetaWarps - 1) / kThetaWarps));
+    // work items: words, hot words split so no item exceeds a quarter of a CTA's share
+    std::vector<culda_item> items, hot;
+    {
+        int64_t it = p->item_tokens;
+        if (it <= 0) it = std::max<int64_t>(1024, std::min<int64_t>(65535, N / ((int64_t)sms * sbps * 4)));
+        ctx->item_tokens = (int)it;
+        int32_t nhot = 0;
+        items = build_items_vec(V, c->word_ptr, ctx->item_tokens, &nhot);
+        if (items.empty() || (int64_t)items.size() >= INT32_MAX) {
+            fail(ctx, CULDA_ERR_FORMAT, "culda_create: no tokens to sample");
+            return bail(CULDA_ERR_FORMAT);
+        }
+        for (const culda_item &x : items)
+            if (x.hot >= 0) hot.push_back(x);
+        ctx->num_items = (int32_t)items.size();
+        ctx->num_hot = nhot;
+        ctx->num_hot_items = (int32_t)hot.size();
+    }
+    ctx->sample_grid = std::max(1, std::min(ctx->num_items, sms * sbps));
+
+    // ---- one device block for every persistent buffer
+    {
+        size_t size = 0;
+        auto add = [&size](size_t bytes) {
+            const size_t off = size;
+            size += (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+            return off;
+        };
+        const size_t o_word_ptr = add(sizeof(int64_t) * ((size_t)V + 1));
+        const size_t o_doc_ptr = add(sizeof(int64_t) * ((size_t)D + 1));
+        const size_t o_doc_ids = add(sizeof(int32_t) * (size_t)N);
+        const size_t o_error = add(64 * sizeof(int32_t));
+        const size_t o_tok_index = reorder ? add(sizeof(int32_t) * (size_t)N) : 0;
+        const size_t o_doc_tok = add(sizeof(int32_t) * (size_t)N);
+        const size_t o_theta = add(sizeof(ThetaEntry) * (size_t)ctx->theta_cap);
+        const size_t o_rows = add(sizeof(int2) * (size_t)D);
+        const size_t o_doc_order = add(sizeof(int32_t) * (size_t)D);
+        const size_t o_items = add(sizeof(culda_item) * items.size());
+        const size_t o_hot_items = add(sizeof(culda_item) * hot.size());
+        const size_t o_hot_phi = add(sizeof(int32_t) * (size_t)ctx->num_hot * K);
+        const size_t o_item_ll = add(sizeof(double) * items.size());
+        const size_t o_seg_start = add(sizeof(int32_t) * (size_t)N);  // at most one segment per token
+        const size_t o_counter = add(64 * sizeof(int32_t));
+        const size_t o_iter = add(sizeof(uint32_t));
+        const size_t o_stats = add(sizeof(DevStats));
+        const size_t o_nk = add(sizeof(int32_t) * (size_t)K);
+        const size_t o_z0 = add(sizeof(uint16_t) * (size_t)N);
+        const size_t o_z1 = add(sizeof(uint16_t) * (size_t)N);
+        const size_t o_zx = add(sizeof(uint16_t) * (size_t)N);
+        const size_t o_u = add(sizeof(float) * (size_t)N);
+        CKB(cudaMalloc((void **)&ctx->d_block, size));
+        char *b = ctx->d_block;
+        ctx->d_word_ptr = reinterpret_cast<int64_t *>(b + o_word_ptr);
+        ctx->d_doc_ptr = reinterpret_cast<int64_t *>(b + o_doc_ptr);
+        ctx->d_doc_ids = reinterpret_cast<int32_t *>(b + o_doc_ids);
+        ctx->d_error = reinterpret_cast<int32_t *>(b + o_error);
+        ctx->d_tok_index = reorder ? reinterpret_cast<int32_t *>(b + o_tok_index) : nullptr;
+        ctx->d_doc_tok = reinterpret_cast<int32_t *>(b + o_doc_tok);
+        ctx->d_theta = reinterpret_cast<ThetaEntry *>(b + o_theta);
+        ctx->d_rows = reinterpret_cast<int2 *>(b + o_rows);
+        ctx->d_doc_order = reinterpret_cast<int32_t *>(b + o_doc_order);
+        ctx->d_items = reinterpret_cast<culda_item *>(b + o_items);
+        ctx->d_hot_items = reinterpret_cast<culda_item *>(b + o_hot_items);
+        ctx->d_hot_phi = reinterpret_cast<int32_t *>(b + o_hot_phi);
+        ctx->d_item_ll = reinterpret_cast<double *>(b + o_item_ll);
+        ctx->d_seg_start = reinterpret_cast<int32_t *>(b + o_seg_start);
+        ctx->d_counter = reinterpret_cast<int32_t *>(b + o_counter);
+        ctx->d_iter = reinterpret_cast<uint32_t *>(b + o_iter);
+        ctx->d_stats = reinterpret_cast<DevStats *>(b + o_stats);
+        ctx->d_nk = reinterpret_cast<int32_t *>(b + o_nk);
+        ctx->d_z[0] = reinterpret_cast<uint16_t *>(b + o_z0);
+        ctx->d_z[1] = reinterpret_cast<uint16_t *>(b + o_z1);
+        ctx->d_zx = reinterpret_cast<uint16_t *>(b + o_zx);
+        ctx->d_u = reinterpret_cast<float *>(b + o_u);
+        ctx->block_bytes = size;
+    }
+
     // corpus upload
-    CKB(dalloc(&ctx->d_word_ptr, (size_t)V + 1));
-    CKB(dalloc(&ctx->d_doc_ptr, (size_t)D + 1));
-    CKB(dalloc(&ctx->d_doc_ids, (size_t)N));
     CKB(cudaMemcpyAsync(ctx->d_word_ptr, c->word_ptr, sizeof(int64_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_doc_ptr, c->doc_ptr, sizeof(int64_t) * ((size_t)D + 1), cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_doc_ids, c->doc_ids, sizeof(int32_t) * (size_t)N, cudaMemcpyHostToDevice, s));
-    CKB(dalloc(&ctx->d_error, 64));
     CKB(cudaMemsetAsync(ctx->d_error, 0, 64 * sizeof(int32_t), s));
+    // the rest of the host layout goes up while the corpus does
+    CKB(cudaMemsetAsync(ctx->d_theta, 0, sizeof(ThetaEntry) * (size_t)std::max<int64_t>(ctx->theta_cap, 1), s));
+    CKB(cudaMemcpyAsync(ctx->d_rows, rows.data(), sizeof(int2) * (size_t)D, cudaMemcpyHostToDevice, s));
+    CKB(cudaMemcpyAsync(ctx->d_doc_order, doc_order.data(), sizeof(int32_t) * (size_t)D, cudaMemcpyHostToDevice, s));
+    CKB(cudaMemcpyAsync(ctx->d_items, items.data(), sizeof(culda_item) * items.size(), cudaMemcpyHostToDevice, s));
+    if (!hot.empty())
+        CKB(cudaMemcpyAsync(ctx->d_hot_items, hot.data(), sizeof(culda_item) * hot.size(), cudaMemcpyHostToDevice, s));
 
-    // doc ids in range and doc lengths consistent with the payload
-    {
-        int32_t *d_cnt = nullptr;
-        CKB(dalloc(&d_cnt, (size_t)D));
-        CKB(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (size_t)D, s));
-        CKB(launch_doc_check(N, D, ctx->d_doc_ids, d_cnt, ctx->d_error, s));
-        std::vector<int32_t> cnt((size_t)D);
-        int32_t e = 0;
-        CKB(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int32_t) * (size_t)D, cudaMemcpyDeviceToHost, s));
-        CKB(cudaMemcpyAsync(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        CKB(cudaStreamSynchronize(s));
-        cudaFree(d_cnt);
-        if (e) {
-            fail(ctx, CULDA_ERR_FORMAT, "culda_create: a doc id is outside [0, %d)", D);
-            return bail(CULDA_ERR_FORMAT);
-        }
-        for (int32_t d = 0; d < D; ++d)
-            if (cnt[d] != c->doc_ptr[d + 1] - c->doc_ptr[d]) {
-                fail(ctx, CULDA_ERR_FORMAT, "culda_create: doc %d has %d tokens in the payload but length %lld", d,
-                     cnt[d], (long long)(c->doc_ptr[d + 1] - c->doc_ptr[d]));
-                return bail(CULDA_ERR_FORMAT);
-            }
-    }
-
-    // Stored token order: inside each word, tokens sorted by their doc's
-    // length, longest first (a stable sort on (word, 65535 - L_d) keeps doc
-    // order among equal lengths).  Neighbouring sampler groups then walk theta
-    // rows of similar length.  Sampling results do not depend on this order:
-    // each token's Philox stream is keyed on its input index.
-    mark("upload, doc check");
     // one arena for the set-up's temporaries: the larger of the token-order
     // sort (8-byte keys in and out, values), the doc-reverse sort and the
     // segment scans (5 int arrays), plus the largest CUB scratch
@@ -687,16 +812,49 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     };
 #define CKA(call)                                                                                              \
     do {                                                                                                       \
-        cudaError_t e_ = (call);                                                                               \
-        if (e_ != cudaSuccess) {                                                                               \
+        const cudaError_t ea_ = (call);                                                                        \
+        if (ea_ != cudaSuccess) {                                                                              \
             arena_free();                                                                                      \
-            CKB(e_);                                                                                           \
+            CKB(ea_);                                                                                          \
         }                                                                                                      \
     } while (0)
-    if (!(p->flags & CULDA_FLAG_NO_REORDER)) {
+
+    // doc ids in range and doc lengths consistent with the payload
+    {
+        arena.reset();
+        int32_t *d_cnt = arena.take<int32_t>((size_t)D);
+        if (!d_cnt) CKA(cudaErrorMemoryAllocation);
+        CKA(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (size_t)D, s));
+        CKA(launch_doc_check(N, D, ctx->d_doc_ids, d_cnt, ctx->d_error, s));
+        std::vector<int32_t> cnt((size_t)D);
+        int32_t e = 0;
+        CKA(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int32_t) * (size_t)D, cudaMemcpyDeviceToHost, s));
+        CKA(cudaMemcpyAsync(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CKA(cudaStreamSynchronize(s));
+        if (e) {
+            arena_free();
+            fail(ctx, CULDA_ERR_FORMAT, "culda_create: a doc id is outside [0, %d)", D);
+            return bail(CULDA_ERR_FORMAT);
+        }
+        for (int32_t d = 0; d < D; ++d)
+            if (cnt[d] != c->doc_ptr[d + 1] - c->doc_ptr[d]) {
+                arena_free();
+                fail(ctx, CULDA_ERR_FORMAT, "culda_create: doc %d has %d tokens in the payload but length %lld", d,
+                     cnt[d], (long long)(c->doc_ptr[d + 1] - c->doc_ptr[d]));
+                return bail(CULDA_ERR_FORMAT);
+            }
+    }
+    mark("upload, doc check");
+
+    // Stored token order: inside each word, tokens sorted by their doc's
+    // length, longest first (a stable sort on (word, 65535 - L_d) keeps doc
+    // order among equal lengths).  Neighbouring segments then walk theta rows
+    // of similar length.  Sampling results do not depend on this order:
+    // each token's Philox stream is keyed on its input index.
+    if (reorder) {
         arena.reset();
         uint64_t *keys = arena.take<uint64_t>((size_t)N), *keys_out = arena.take<uint64_t>((size_t)N);
-        int32_t *vals = arena.take<int32_t>((size_t)N), *ids2 = nullptr;
+        int32_t *vals = arena.take<int32_t>((size_t)N);
         int end_bit = 17;
         while ((1ll << (end_bit - 16)) < (int64_t)V) ++end_bit;
         size_t tmp_bytes = 0;
@@ -704,16 +862,14 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
                                             end_bit, s));
         void *tmp = arena.take<char>(tmp_bytes);
         if (!keys || !keys_out || !vals || !tmp) CKA(cudaErrorMemoryAllocation);
-        CKA(dalloc(&ctx->d_tok_index, (size_t)N));
         CKA(launch_order_keys(V, N, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, keys, s));
         CKA(launch_iota(N, vals, s));
         CKA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
                                             end_bit, s));
-        CKA(dalloc(&ids2, (size_t)N));
+        // the doc ids in the stored order, through the (now free) key buffer
+        int32_t *ids2 = reinterpret_cast<int32_t *>(keys);
         CKA(launch_gather<int32_t>(N, ctx->d_tok_index, ctx->d_doc_ids, ids2, s));
-        CKA(cudaStreamSynchronize(s));
-        cudaFree(ctx->d_doc_ids);
-        ctx->d_doc_ids = ids2;
+        CKA(cudaMemcpyAsync(ctx->d_doc_ids, ids2, sizeof(int32_t) * (size_t)N, cudaMemcpyDeviceToDevice, s));
     }
 
     mark("token order sort");
@@ -721,7 +877,6 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     // (the reference builds it on the host, doc_chunk.cpp:225-255)
     {
         arena.reset();
-        CKA(dalloc(&ctx->d_doc_tok, (size_t)N));
         int32_t *keys_out = arena.take<int32_t>((size_t)N), *vals_in = arena.take<int32_t>((size_t)N);
         int end_bit = 1;
         while ((1ll << end_bit) < (int64_t)D) ++end_bit;
@@ -734,98 +889,17 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         CKA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok, (int)N,
                                             0, end_bit, s));
     }
-
     mark("doc-reverse sort");
-    // theta layout: capacity roundup32(min(L_d, K)) per doc (model_theta.cpp:50-56)
-    ctx->h_doc_ptr.assign(c->doc_ptr, c->doc_ptr + D + 1);
-    ctx->h_max_ia.resize((size_t)D + 1);
-    std::vector<int2> rows((size_t)D);
-    int64_t off = 0;
-    for (int32_t d = 0; d < D; ++d) {
-        int64_t len = c->doc_ptr[d + 1] - c->doc_ptr[d];
-        if (len > K) len = K;
-        len = (len + 31) / 32 * 32;
-        if (off + len >= (int64_t)INT32_MAX) {
-            fail(ctx, CULDA_ERR_UNSUPPORTED, "culda_create: theta capacity exceeds int32 offsets");
-            return bail(CULDA_ERR_UNSUPPORTED);
-        }
-        ctx->h_max_ia[d] = (int32_t)off;
-        rows[d] = make_int2((int)off, (int)off);
-        off += len;
-        ctx->doc_term += (double)(c->doc_ptr[d + 1] - c->doc_ptr[d]) *
-                         std::log((double)(c->doc_ptr[d + 1] - c->doc_ptr[d]) + (double)K * (double)p->alpha);
-    }
-    ctx->h_max_ia[D] = (int32_t)off;
-    ctx->theta_cap = off;
-    CKB(dalloc(&ctx->d_theta, (size_t)off));
-    CKB(cudaMemsetAsync(ctx->d_theta, 0, sizeof(ThetaEntry) * (size_t)std::max<int64_t>(off, 1), s));
-    CKB(dalloc(&ctx->d_rows, (size_t)D));
-    CKB(cudaMemcpyAsync(ctx->d_rows, rows.data(), sizeof(int2) * (size_t)D, cudaMemcpyHostToDevice, s));
-
-    // docs longest first for the theta rebuild's warps: a counting sort on
-    // the length (below 65536), stable in doc id
-    {
-        std::vector<int32_t> order((size_t)D), start(65537, 0);
-        for (int32_t d = 0; d < D; ++d) start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d])) + 1]++;
-        for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
-        for (int32_t d = 0; d < D; ++d) order[(size_t)start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d]))]++] = d;
-        CKB(dalloc(&ctx->d_doc_order, (size_t)D));
-        CKB(cudaMemcpyAsync(ctx->d_doc_order, order.data(), sizeof(int32_t) * (size_t)D, cudaMemcpyHostToDevice, s));
-        CKB(cudaStreamSynchronize(s));
-    }
-
-    mark("theta layout, order");
-    // grids
-    const int sms = num_sms(ctx->device);
-    int sbps = sample_blocks_per_sm(K, gl, sb);
-    if (sbps <= 0) {
-        fail(ctx, CULDA_ERR_CUDA, "culda_create: sampler does not fit on the device for K=%d", K);
-        return bail(CULDA_ERR_CUDA);
-    }
-    int tbps = theta_blocks_per_sm(K);
-    if (tbps <= 0) tbps = 1;
-    ctx->theta_grid = std::max(1, std::min(sms * tbps, (D + kThetaWarps - 1) / kThetaWarps));
-
-    // work items: words, hot words split so no item exceeds a quarter of a CTA's share
-    {
-        int64_t it = p->item_tokens;
-        if (it <= 0) it = std::max<int64_t>(1024, std::min<int64_t>(65535, N / ((int64_t)sms * sbps * 4)));
-        ctx->item_tokens = (int)it;
-        int32_t nhot = 0;
-        const std::vector<culda_item> items = build_items_vec(V, c->word_ptr, ctx->item_tokens, &nhot);
-        const int64_t n_items = (int64_t)items.size();
-        if (n_items <= 0 || n_items >= INT32_MAX) {
-            fail(ctx, CULDA_ERR_FORMAT, "culda_create: no tokens to sample");
-            return bail(CULDA_ERR_FORMAT);
-        }
-        std::vector<culda_item> hot;
-        for (const culda_item &x : items)
-            if (x.hot >= 0) hot.push_back(x);
-        ctx->num_items = (int32_t)n_items;
-        ctx->num_hot = nhot;
-        ctx->num_hot_items = (int32_t)hot.size();
-        CKB(dalloc(&ctx->d_items, items.size()));
-        CKB(cudaMemcpyAsync(ctx->d_items, items.data(), sizeof(culda_item) * items.size(), cudaMemcpyHostToDevice, s));
-        CKB(dalloc(&ctx->d_hot_items, hot.size()));
-        if (!hot.empty())
-            CKB(cudaMemcpyAsync(ctx->d_hot_items, hot.data(), sizeof(culda_item) * hot.size(), cudaMemcpyHostToDevice,
-                                s));
-        CKB(dalloc(&ctx->d_hot_phi, (size_t)nhot * K));
-        CKB(dalloc(&ctx->d_item_ll, (size_t)n_items));
-        CKB(cudaStreamSynchronize(s));
-    }
-    ctx->sample_grid = std::max(1, std::min(ctx->num_items, sms * sbps));
-    mark("work items");
     rc = build_segments_device(ctx, arena);
     arena_free();
 #undef CKA
     if (rc) return bail(rc);
 
-    CKB(dalloc(&ctx->d_counter, 64));
-    CKB(dalloc(&ctx->d_iter, 1));
-    CKB(dalloc(&ctx->d_stats, 1));
-    CKB(dalloc(&ctx->d_nk, (size_t)K));
-    CKB(cudaMallocHost((void **)&ctx->h_stats, sizeof(DevStats)));
+    ctx->h_stats = pinned_stats_get();
+    if (!ctx->h_stats) {
+        fail(ctx, CULDA_ERR_OOM, "culda_create: pinned host memory for the iteration statistics");
+        return bail(CULDA_ERR_OOM);
+    }
     memset(ctx->h_stats, 0, sizeof(DevStats));
     CKB(cudaMemsetAsync(ctx->d_stats, 0, sizeof(DevStats), s));
     const uint32_t one = 1;
@@ -833,10 +907,6 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
 
     mark("segments");
     // topics: Philox init, then the initial counts (SingleChunkSingleGPU.h:24-41)
-    CKB(dalloc(&ctx->d_z[0], (size_t)N));
-    CKB(dalloc(&ctx->d_z[1], (size_t)N));
-    CKB(dalloc(&ctx->d_zx, (size_t)N));
-    CKB(dalloc(&ctx->d_u, (size_t)N));
     CKB(launch_init_topics(N, K, p->seed, ctx->d_tok_index, ctx->d_z[0], s));
     ctx->cur = 0;
     rc = rebuild_counts(ctx);
@@ -1077,11 +1147,11 @@ extern "C" int culda_get_info(const culda_ctx *ctx, culda_info *info) {
     info->kernels_per_iteration = (ctx->num_hot > 0 ? 1 : 0) + 5;
     info->theta_capacity = ctx->theta_cap;
     const int64_t N = ctx->N, D = ctx->D, V = ctx->V, K = ctx->K;
-    info->device_bytes = 8 * (V + 1) + 8 * (D + 1) + 4 * N /*doc ids*/ + 4 * N /*doc_tok*/ + 4 * D /*order*/ +
-                         (ctx->d_tok_index ? 4 * N : 0) + 3 * 2 * N /*topics x2 + copy buffer*/ + 4 * N /*uniforms*/ +
-                         (int64_t)sizeof(ThetaEntry) * ctx->theta_cap + 8 * D /*rows*/ + 4 * K +
-                         (int64_t)sizeof(culda_item) * (ctx->num_items + ctx->num_hot_items) + 4 * ctx->num_segs +
-                         4 * (int64_t)ctx->num_hot * K + 8 * (int64_t)ctx->num_items;
+    (void)N;
+    (void)D;
+    (void)V;
+    (void)K;
+    info->device_bytes = (int64_t)ctx->block_bytes;
     info->doc_term = ctx->doc_term;
     return CULDA_OK;
 }
@@ -1106,15 +1176,8 @@ extern "C" void culda_destroy(culda_ctx *ctx) {
     free_learned_state(ctx);
     for (int c = 0; c < 2; ++c)
         if (ctx->graph[c]) cudaGraphExecDestroy(ctx->graph[c]);
-    void *bufs[] = {ctx->d_word_ptr, ctx->d_doc_ptr, ctx->d_doc_ids,  ctx->d_doc_tok,  ctx->d_doc_order,
-                    ctx->d_tok_index, ctx->d_zx,     ctx->d_u,
-                    ctx->d_z[0],     ctx->d_z[1],    ctx->d_theta,    ctx->d_rows,     ctx->d_nk,
-                    ctx->d_items,    ctx->d_hot_items, ctx->d_hot_phi, ctx->d_item_ll, ctx->d_counter,
-                    ctx->d_seg_start,
-                    ctx->d_iter,     ctx->d_stats,   ctx->d_error};
-    for (void *b : bufs)
-        if (b) cudaFree(b);
-    if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+    if (ctx->d_block) cudaFree(ctx->d_block);
+    if (ctx->h_stats) pinned_stats_put(ctx->h_stats);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->ev_s0, ctx->ev_s1, ctx->ev_t0, ctx->ev_t1})
         if (ev) cudaEventDestroy(ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

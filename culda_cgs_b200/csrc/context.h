@@ -47,7 +47,9 @@ struct culda_ctx {
     uint32_t *d_iter = nullptr;
     culda::DevStats *d_stats = nullptr;
     int32_t *d_error = nullptr;
-    culda::DevStats *h_stats = nullptr;  // pinned
+    culda::DevStats *h_stats = nullptr;  // pinned (a slot of the process-wide pool)
+    char *d_block = nullptr;             // every buffer above that culda_create allocates, in one allocation
+    size_t block_bytes = 0;
 
     int sample_grid = 1, theta_grid = 1;
     double doc_term = 0;  // sum_d L_d * log(L_d + K alpha)

@@ -216,7 +216,8 @@ constexpr uint32_t kTuneIteration = 3;
 // uniforms once, then per variant one warm-up and two timed launches that
 // write the other topic buffer.  The context's state does not change.
 int autotune_sampler(culda_ctx *ctx) {
-    static const int kCands[][2] = {{kFlatLanes, kSampleBlocksDefault}, {4, kSampleBlocksHigh},
+    static const int kCands[][2] = {{kFlatLanes, kSampleBlocksDefault}, {kFlatLanes, kSampleBlocksHigh},
+                                    {4, kSampleBlocksHigh},
                                     {8, kSampleBlocksHigh},                {16, kSampleBlocksHigh},
                                     {2, kSampleBlocksDefault},             {4, kSampleBlocksDefault},
                                     {8, kSampleBlocksDefault}};
@@ -412,16 +413,17 @@ namespace {
 
 constexpr int kSegmentMax = 32;  // tokens per segment (bounds the work of one group on one row)
 
-__global__ void mark_items_kernel(const culda_item *__restrict__ items, int num_items, int32_t *mark) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_items; i += gridDim.x * blockDim.x)
-        mark[items[i].begin] = 1;
+// key[t] = t where a run of one doc starts (doc change), else 0; item starts
+// are added by item_keys_kernel
+__global__ void run_key_kernel(int64_t n, const int32_t *__restrict__ doc_ids, int32_t *key) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        key[t] = (t == 0 || doc_ids[t] != doc_ids[t - 1]) ? (int32_t)t : 0;
 }
 
-// key[t] = t where a run of one doc starts (item start or doc change), else 0
-__global__ void run_key_kernel(int64_t n, const int32_t *__restrict__ doc_ids, const int32_t *__restrict__ mark,
-                               int32_t *key) {
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-        key[t] = (t == 0 || mark[t] || doc_ids[t] != doc_ids[t - 1]) ? (int32_t)t : 0;
+// every item starts a run
+__global__ void item_keys_kernel(const culda_item *__restrict__ items, int num_items, int32_t *key) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_items; i += gridDim.x * blockDim.x)
+        key[items[i].begin] = (int32_t)items[i].begin;
 }
 
 struct MaxOp {
@@ -448,9 +450,6 @@ __global__ void item_segments_kernel(culda_item *items, int num_items, const int
     }
 }
 
-// One device buffer for the set-up's temporaries (sort keys and values, scan
-// arrays, CUB scratch), carved by a bump allocator and released once: set-up
-// makes one allocation and one free instead of one pair per temporary.
 // A process-wide pool of pinned DevStats slots: a cudaMallocHost costs
 // milliseconds, so contexts take slots from shared pinned pages and give them
 // back on destroy (the pages live as long as the process).
@@ -475,9 +474,19 @@ void pinned_stats_put(DevStats *p) {
     g_pinned_free.push_back(p);
 }
 
+// Device space for the set-up's temporaries (sort keys and values, scan
+// arrays, CUB scratch), carved by a bump allocator.  It is either a region of
+// the context's block whose buffers are not used until set-up ends (owned =
+// false) or, when that region is too small, one allocation of its own.
 struct SetupArena {
     char *base = nullptr;
     size_t size = 0, used = 0;
+    bool owned = false;
+    void use(char *b, size_t s) {
+        base = b;
+        size = s;
+        used = 0;
+    }
     template <class T>
     T *take(size_t n) {
         const size_t bytes = (std::max<size_t>(n, 1) * sizeof(T) + 255) & ~(size_t)255;
@@ -489,16 +498,12 @@ struct SetupArena {
     void reset() { used = 0; }
 };
 
-size_t arena_bytes(size_t n_items_of_4_bytes, size_t scratch) { return n_items_of_4_bytes * 4 + scratch + 16 * 256; }
 
 // Segments of the stored token order, on the device (see culda_build_segments).
 int build_segments_device(culda_ctx *ctx, SetupArena &arena) {
     cudaStream_t s = ctx->stream;
     const int64_t N = ctx->N;
-    int32_t *mark = nullptr, *key = nullptr, *run = nullptr, *flag = nullptr, *index = nullptr;
-    void *tmp = nullptr;
     size_t tmp_bytes = 0, b2 = 0;
-    arena.reset();
     int rc = CULDA_OK;
     auto grid = [](int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); };
     do {
@@ -510,37 +515,30 @@ int build_segments_device(culda_ctx *ctx, SetupArena &arena) {
             break;                                                                                         \
         }                                                                                                  \
     }
-        mark = arena.take<int32_t>((size_t)N);
-        key = arena.take<int32_t>((size_t)N);
-        run = arena.take<int32_t>((size_t)N);
-        flag = arena.take<int32_t>((size_t)N + 1);
-        index = arena.take<int32_t>((size_t)N + 1);
-        if (!mark || !key || !run || !flag || !index) {
+        // two arrays: A holds the run keys, then the segment flags; B the run
+        // starts, then the flags' exclusive prefix (the segment index)
+        int32_t *A = arena.take<int32_t>((size_t)N + 1), *B = arena.take<int32_t>((size_t)N + 1);
+        CKS(cub::DeviceScan::InclusiveScan(nullptr, tmp_bytes, A, B, MaxOp(), (int)N, s));
+        CKS(cub::DeviceScan::ExclusiveSum(nullptr, b2, A, B, (int)N + 1, s));
+        void *tmp = arena.take<char>(std::max(tmp_bytes, b2));
+        if (!A || !B || !tmp) {
             rc = fail(ctx, CULDA_ERR_OOM, "segments: set-up arena too small");
             break;
         }
-        CKS(cudaMemsetAsync(mark, 0, sizeof(int32_t) * (size_t)N, s));
-        mark_items_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, mark);
-        run_key_kernel<<<grid(N), 256, 0, s>>>(N, ctx->d_doc_ids, mark, key);
-        CKS(cudaGetLastError());
-        CKS(cub::DeviceScan::InclusiveScan(nullptr, tmp_bytes, key, run, MaxOp(), (int)N, s));
-        CKS(cub::DeviceScan::ExclusiveSum(nullptr, b2, flag, index, (int)N + 1, s));
         tmp_bytes = std::max(tmp_bytes, b2);
-        tmp = arena.take<char>(tmp_bytes);
-        if (!tmp) {
-            rc = fail(ctx, CULDA_ERR_OOM, "segments: set-up arena too small");
-            break;
-        }
-        CKS(cub::DeviceScan::InclusiveScan(tmp, tmp_bytes, key, run, MaxOp(), (int)N, s));
-        seg_flag_kernel<<<grid(N + 1), 256, 0, s>>>(N, run, flag);
+        run_key_kernel<<<grid(N), 256, 0, s>>>(N, ctx->d_doc_ids, A);
+        item_keys_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, A);
         CKS(cudaGetLastError());
-        CKS(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, flag, index, (int)N + 1, s));
+        CKS(cub::DeviceScan::InclusiveScan(tmp, tmp_bytes, A, B, MaxOp(), (int)N, s));
+        seg_flag_kernel<<<grid(N + 1), 256, 0, s>>>(N, B, A);
+        CKS(cudaGetLastError());
+        CKS(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, A, B, (int)N + 1, s));
         int32_t total = 0;
-        CKS(cudaMemcpyAsync(&total, index + N, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CKS(cudaMemcpyAsync(&total, B + N, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         CKS(cudaStreamSynchronize(s));
         ctx->num_segs = total;  // d_seg_start holds one entry per token, the most there can be
-        seg_scatter_kernel<<<grid(N), 256, 0, s>>>(N, flag, index, ctx->d_seg_start);
-        item_segments_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, index);
+        seg_scatter_kernel<<<grid(N), 256, 0, s>>>(N, A, B, ctx->d_seg_start);
+        item_segments_kernel<<<grid(ctx->num_items), 256, 0, s>>>(ctx->d_items, ctx->num_items, B);
         CKS(cudaGetLastError());
         CKS(cudaStreamSynchronize(s));
 #undef CKS
@@ -605,7 +603,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     int rc = CULDA_OK;
     SetupArena arena;  // the set-up's temporaries (sorts, segment scans)
     auto bail = [&](int code) {
-        if (arena.base) cudaFree(arena.base);
+        if (arena.owned && arena.base) cudaFree(arena.base);
         culda_destroy(ctx);
         return code;
     };
@@ -716,12 +714,35 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     }
     ctx->sample_grid = std::max(1, std::min(ctx->num_items, sms * sbps));
 
-    // ---- one device block for every persistent buffer
+    // ---- one device block for every persistent buffer.  The buffers that
+    // set-up does not touch until its end (doc-reverse index, segment starts,
+    // topics, uniforms, theta) come last: while the sorts and scans run, that
+    // region holds their temporaries instead of an allocation of its own.
+    auto rnd = [](size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255; };
+    size_t t_order = 0, t_doc = 0, t_scan = 0, t_sum = 0;
+    int order_bits = 17, doc_bits = 1;
+    while ((1ll << (order_bits - 16)) < (int64_t)V) ++order_bits;
+    while ((1ll << doc_bits) < (int64_t)D) ++doc_bits;
+    CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_order, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                        (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, order_bits, s));
+    CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_doc, (const int32_t *)nullptr, (int32_t *)nullptr,
+                                        (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, doc_bits, s));
+    CKB(cub::DeviceScan::InclusiveScan(nullptr, t_scan, (const int32_t *)nullptr, (int32_t *)nullptr, MaxOp(), (int)N,
+                                       s));
+    CKB(cub::DeviceScan::ExclusiveSum(nullptr, t_sum, (const int32_t *)nullptr, (int32_t *)nullptr, (int)N + 1, s));
+    // what each set-up phase takes from the arena (SetupArena rounds like rnd)
+    const size_t need_check = rnd(sizeof(int32_t) * (size_t)D);
+    const size_t need_order = reorder ? 2 * rnd(sizeof(uint64_t) * (size_t)N) + rnd(sizeof(int32_t) * (size_t)N) +
+                                            rnd(t_order)
+                                      : 0;
+    const size_t need_rev = 2 * rnd(sizeof(int32_t) * (size_t)N) + rnd(t_doc);
+    const size_t need_seg = 2 * rnd(sizeof(int32_t) * ((size_t)N + 1)) + rnd(std::max(t_scan, t_sum));
+    size_t o_late = 0, o_after_doc_tok = 0, o_after_seg = 0;
     {
         size_t size = 0;
-        auto add = [&size](size_t bytes) {
+        auto add = [&size, &rnd](size_t bytes) {
             const size_t off = size;
-            size += (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+            size += rnd(bytes);
             return off;
         };
         const size_t o_word_ptr = add(sizeof(int64_t) * ((size_t)V + 1));
@@ -729,23 +750,27 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         const size_t o_doc_ids = add(sizeof(int32_t) * (size_t)N);
         const size_t o_error = add(64 * sizeof(int32_t));
         const size_t o_tok_index = reorder ? add(sizeof(int32_t) * (size_t)N) : 0;
-        const size_t o_doc_tok = add(sizeof(int32_t) * (size_t)N);
-        const size_t o_theta = add(sizeof(ThetaEntry) * (size_t)ctx->theta_cap);
         const size_t o_rows = add(sizeof(int2) * (size_t)D);
         const size_t o_doc_order = add(sizeof(int32_t) * (size_t)D);
         const size_t o_items = add(sizeof(culda_item) * items.size());
         const size_t o_hot_items = add(sizeof(culda_item) * hot.size());
         const size_t o_hot_phi = add(sizeof(int32_t) * (size_t)ctx->num_hot * K);
         const size_t o_item_ll = add(sizeof(double) * items.size());
-        const size_t o_seg_start = add(sizeof(int32_t) * (size_t)N);  // at most one segment per token
         const size_t o_counter = add(64 * sizeof(int32_t));
         const size_t o_iter = add(sizeof(uint32_t));
         const size_t o_stats = add(sizeof(DevStats));
         const size_t o_nk = add(sizeof(int32_t) * (size_t)K);
+        // the region set-up borrows, in the order it gives the buffers back
+        const size_t o_doc_tok = add(sizeof(int32_t) * (size_t)N);
+        const size_t o_seg_start = add(sizeof(int32_t) * (size_t)N);  // at most one segment per token
         const size_t o_z0 = add(sizeof(uint16_t) * (size_t)N);
         const size_t o_z1 = add(sizeof(uint16_t) * (size_t)N);
         const size_t o_zx = add(sizeof(uint16_t) * (size_t)N);
         const size_t o_u = add(sizeof(float) * (size_t)N);
+        const size_t o_theta = add(sizeof(ThetaEntry) * (size_t)ctx->theta_cap);
+        o_late = o_doc_tok;
+        o_after_doc_tok = o_seg_start;
+        o_after_seg = o_z0;
         CKB(cudaMalloc((void **)&ctx->d_block, size));
         char *b = ctx->d_block;
         ctx->d_word_ptr = reinterpret_cast<int64_t *>(b + o_word_ptr);
@@ -772,6 +797,24 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         ctx->d_u = reinterpret_cast<float *>(b + o_u);
         ctx->block_bytes = size;
     }
+    // the borrowed region serves every phase when it is large enough (theta's
+    // capacity is at least about half the token count); otherwise set-up
+    // allocates an arena of its own
+    const size_t size = ctx->block_bytes;
+    const bool borrow = std::max(need_check, need_order) <= size - o_late && need_rev <= size - o_after_doc_tok &&
+                        need_seg <= size - o_after_seg;
+    if (!borrow) {
+        arena.size = std::max(std::max(need_check, need_order), std::max(need_rev, need_seg));
+        CKB(cudaMalloc((void **)&arena.base, arena.size));
+        arena.owned = true;
+    }
+    // the arena for a phase that may use the block from offset `from` on
+    auto arena_at = [&](size_t from) {
+        if (arena.owned)
+            arena.reset();
+        else
+            arena.use(ctx->d_block + from, size - from);
+    };
 
     // corpus upload
     CKB(cudaMemcpyAsync(ctx->d_word_ptr, c->word_ptr, sizeof(int64_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, s));
@@ -779,36 +822,16 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     CKB(cudaMemcpyAsync(ctx->d_doc_ids, c->doc_ids, sizeof(int32_t) * (size_t)N, cudaMemcpyHostToDevice, s));
     CKB(cudaMemsetAsync(ctx->d_error, 0, 64 * sizeof(int32_t), s));
     // the rest of the host layout goes up while the corpus does
-    CKB(cudaMemsetAsync(ctx->d_theta, 0, sizeof(ThetaEntry) * (size_t)std::max<int64_t>(ctx->theta_cap, 1), s));
     CKB(cudaMemcpyAsync(ctx->d_rows, rows.data(), sizeof(int2) * (size_t)D, cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_doc_order, doc_order.data(), sizeof(int32_t) * (size_t)D, cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_items, items.data(), sizeof(culda_item) * items.size(), cudaMemcpyHostToDevice, s));
     if (!hot.empty())
         CKB(cudaMemcpyAsync(ctx->d_hot_items, hot.data(), sizeof(culda_item) * hot.size(), cudaMemcpyHostToDevice, s));
 
-    // one arena for the set-up's temporaries: the larger of the token-order
-    // sort (8-byte keys in and out, values), the doc-reverse sort and the
-    // segment scans (5 int arrays), plus the largest CUB scratch
-    {
-        int end_bit = 17;
-        while ((1ll << (end_bit - 16)) < (int64_t)V) ++end_bit;
-        size_t t_order = 0, t_doc = 0, t_scan = 0, t_sum = 0;
-        CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_order, (const uint64_t *)nullptr, (uint64_t *)nullptr,
-                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, end_bit, s));
-        CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_doc, (const int32_t *)nullptr, (int32_t *)nullptr,
-                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, 31, s));
-        CKB(cub::DeviceScan::InclusiveScan(nullptr, t_scan, (const int32_t *)nullptr, (int32_t *)nullptr, MaxOp(),
-                                           (int)N, s));
-        CKB(cub::DeviceScan::ExclusiveSum(nullptr, t_sum, (const int32_t *)nullptr, (int32_t *)nullptr, (int)N + 1,
-                                          s));
-        const size_t words = std::max<size_t>(5 * (size_t)N, 5 * ((size_t)N + 2));
-        const size_t scratch = std::max(std::max(t_order, t_doc), std::max(t_scan, t_sum));
-        arena.size = arena_bytes(words, scratch);
-        CKB(cudaMalloc((void **)&arena.base, arena.size));
-    }
     auto arena_free = [&]() {
-        if (arena.base) cudaFree(arena.base);
+        if (arena.owned && arena.base) cudaFree(arena.base);
         arena.base = nullptr;
+        arena.owned = false;
     };
 #define CKA(call)                                                                                              \
     do {                                                                                                       \
@@ -821,7 +844,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
 
     // doc ids in range and doc lengths consistent with the payload
     {
-        arena.reset();
+        arena_at(o_late);
         int32_t *d_cnt = arena.take<int32_t>((size_t)D);
         if (!d_cnt) CKA(cudaErrorMemoryAllocation);
         CKA(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (size_t)D, s));
@@ -852,11 +875,10 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     // of similar length.  Sampling results do not depend on this order:
     // each token's Philox stream is keyed on its input index.
     if (reorder) {
-        arena.reset();
+        arena_at(o_late);
         uint64_t *keys = arena.take<uint64_t>((size_t)N), *keys_out = arena.take<uint64_t>((size_t)N);
         int32_t *vals = arena.take<int32_t>((size_t)N);
-        int end_bit = 17;
-        while ((1ll << (end_bit - 16)) < (int64_t)V) ++end_bit;
+        const int end_bit = order_bits;
         size_t tmp_bytes = 0;
         CKA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
                                             end_bit, s));
@@ -876,10 +898,9 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     // doc-reverse index: stable radix sort of stored token positions by doc id
     // (the reference builds it on the host, doc_chunk.cpp:225-255)
     {
-        arena.reset();
+        arena_at(o_after_doc_tok);
         int32_t *keys_out = arena.take<int32_t>((size_t)N), *vals_in = arena.take<int32_t>((size_t)N);
-        int end_bit = 1;
-        while ((1ll << end_bit) < (int64_t)D) ++end_bit;
+        const int end_bit = doc_bits;
         size_t tmp_bytes = 0;
         CKA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, ctx->d_doc_ids, keys_out, vals_in, ctx->d_doc_tok,
                                             (int)N, 0, end_bit, s));
@@ -890,10 +911,13 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
                                             0, end_bit, s));
     }
     mark("doc-reverse sort");
+    arena_at(o_after_seg);
     rc = build_segments_device(ctx, arena);
     arena_free();
 #undef CKA
     if (rc) return bail(rc);
+    // theta's storage held set-up temporaries until now
+    CKB(cudaMemsetAsync(ctx->d_theta, 0, sizeof(ThetaEntry) * (size_t)std::max<int64_t>(ctx->theta_cap, 1), s));
 
     ctx->h_stats = pinned_stats_get();
     if (!ctx->h_stats) {

@@ -68,7 +68,7 @@ inline int pow2_ceil(int k) {
 // Sampler variants: lanes per token G and the register budget, given as the
 // resident CTAs per SM the kernel is compiled for (kSampleBlocksDefault for
 // every G; kSampleBlocksHigh for G = 4, 8, 16).  G = kFlatLanes is the
-// warp-flattened walk (kSampleBlocksDefault only).
+// warp-flattened walk (either register budget).
 constexpr int kSampleBlocksDefault = 8;
 constexpr int kSampleBlocksHigh = 10;
 constexpr int kFlatLanes = -1;

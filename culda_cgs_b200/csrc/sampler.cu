@@ -801,9 +801,11 @@ static const void *sample_fn() {
 }
 
 static const void *sample_kernel_for(int g, int minb) {
-    if (g == kFlatLanes)
-        return minb == kSampleBlocksDefault ? reinterpret_cast<const void *>(&sample_flat_kernel<kSampleBlocksDefault>)
-                                            : nullptr;
+    if (g == kFlatLanes) {
+        if (minb == kSampleBlocksDefault) return reinterpret_cast<const void *>(&sample_flat_kernel<kSampleBlocksDefault>);
+        if (minb == kSampleBlocksHigh) return reinterpret_cast<const void *>(&sample_flat_kernel<kSampleBlocksHigh>);
+        return nullptr;
+    }
     if (minb == kSampleBlocksDefault) switch (g) {
             case 1: return sample_fn<1, kSampleBlocksDefault>();
             case 2: return sample_fn<2, kSampleBlocksDefault>();

@@ -180,7 +180,8 @@ typedef struct culda_params {
     int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto, at most 65535 */
     int32_t flags;        /* CULDA_FLAG_* */
     int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (8),
-                              8 (<= 64 registers), or 10 (<= 48 registers; group_lanes 4, 8, 16) */
+                              8 (<= 64 registers), or 10 (<= 48 registers; the flat walk and
+                              group_lanes 4, 8, 16) */
 } culda_params;
 
 /* group_lanes value of the warp-flattened sampler: a warp splits the rows of up

@@ -74,6 +74,7 @@ CASES = [  # name, corpus, K, lanes per token, item tokens (0 = auto), sampler r
     ("mini-k1024-flat-hot", MINI.gen, 1024, -1, 300, 0),
     ("mini-k256-flat", MINI.gen, 256, -1, 0, 0),
     ("mini-k4096-flat", MINI.gen, 4096, -1, 0, 0),
+    ("mini-k1024-flat-b10-hot", MINI.gen, 1024, -1, 300, 10),
 ]
 
 
@@ -112,6 +113,21 @@ def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens, 
         assert_ll_close(ll_gpu, ll_ora)
         # the snapshot draw left the state untouched
         assert np.array_equal(m.topics(), s.z)
+
+
+def test_input_token_order_matches_the_oracle(corpora):
+    """CULDA_FLAG_NO_REORDER keeps tokens in input order (no token index):
+    the counts and draws still match the oracle."""
+    c = corpora[id(MINI.gen)]
+    seed = 4321
+    with cb.LDA(c, 1024, 50.0 / 1024, 0.01, seed=seed, flags=cb.CULDA_FLAG_NO_REORDER) as m:
+        s0 = assert_counts_exact(m, c)
+        z1_ora, margin, ll0 = s0.sample(seed, 1)
+        st = m.iterate(1)[0]
+        assert st["status"] == 0
+        assert_ll_close(st["loglik"], ll0)
+        assert_draws_match(m.topics(), z1_ora, margin)
+        assert_counts_exact(m, c)
 
 
 @pytest.mark.parametrize("g,blocks", [(1, 8), (4, 8), (8, 8), (32, 8), (8, 10), (-1, 8)])

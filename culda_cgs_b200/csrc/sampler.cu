@@ -448,7 +448,9 @@ constexpr int kFlatMeta = 2 * (kFlatSegs + 1) + 4 * kFlatSegs;  // ints of per-w
 constexpr int kWalkLanes = 4;                     // lanes walking one range: 4 units, 128 bytes, per step
 
 // Units of one warp batch: at least a whole row of K entries (K / 8 units).
-__host__ __device__ constexpr int flat_unit_budget(int k) { return k / kUnit > 256 ? k / kUnit : 256; }
+// 512 (4,096 entries, 2 KB of prefixes per warp) was the fastest of 256, 512
+// and 1024 on the 60M-token and the uneven 118M-token workloads.
+__host__ __device__ constexpr int flat_unit_budget(int k) { return k / kUnit > 512 ? k / kUnit : 512; }
 
 __device__ __forceinline__ Step load_unit(const ThetaEntry *__restrict__ theta, int idx) {
     Step st;

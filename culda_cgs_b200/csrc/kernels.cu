@@ -54,15 +54,28 @@ __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
             if (lane == 0) atomicOr(error, kErrLongDoc);
             continue;
         }
-        for (int64_t j = b + lane; j < e; j += 32) {
-            const uint32_t z = topics[doc_tok[j]];
-            if (z >= (uint32_t)K) {
-                atomicOr(error, kErrTopicRange);
-                continue;
+        // four tokens per lane in flight: the index loads, then the topic
+        // loads they address, then the histogram updates
+        constexpr int kInFlight = 4;
+        for (int64_t j0 = b + lane; j0 < e; j0 += 32 * kInFlight) {
+            int32_t idx[kInFlight];
+            uint32_t zz[kInFlight];
+#pragma unroll
+            for (int u = 0; u < kInFlight; ++u) idx[u] = j0 + 32 * u < e ? doc_tok[j0 + 32 * u] : -1;
+#pragma unroll
+            for (int u = 0; u < kInFlight; ++u) zz[u] = idx[u] >= 0 ? (uint32_t)topics[idx[u]] : 0u;
+#pragma unroll
+            for (int u = 0; u < kInFlight; ++u) {
+                if (idx[u] < 0) continue;
+                const uint32_t z = zz[u];
+                if (z >= (uint32_t)K) {
+                    atomicOr(error, kErrTopicRange);
+                    continue;
+                }
+                const uint32_t sh = (z & 1u) << 4;
+                const uint32_t old = atomicAdd(&cnt[z >> 1], 1u << sh);
+                if (((old >> sh) & 0xFFFFu) == 0u) atomicOr(&mask[z >> 5], 1u << (z & 31u));
             }
-            const uint32_t sh = (z & 1u) << 4;
-            const uint32_t old = atomicAdd(&cnt[z >> 1], 1u << sh);
-            if (((old >> sh) & 0xFFFFu) == 0u) atomicOr(&mask[z >> 5], 1u << (z & 31u));
         }
         __syncwarp();
         const int2 row = rows[d];

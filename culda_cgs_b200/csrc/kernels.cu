@@ -54,9 +54,9 @@ __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
             if (lane == 0) atomicOr(error, kErrLongDoc);
             continue;
         }
-        // four tokens per lane in flight: the index loads, then the topic
+        // eight tokens per lane in flight: the index loads, then the topic
         // loads they address, then the histogram updates
-        constexpr int kInFlight = 4;
+        constexpr int kInFlight = 8;
         for (int64_t j0 = b + lane; j0 < e; j0 += 32 * kInFlight) {
             int32_t idx[kInFlight];
             uint32_t zz[kInFlight];

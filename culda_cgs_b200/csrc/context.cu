@@ -674,16 +674,6 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
                 ctx->doc_term +=
                     (double)docs_of_len[len] * (double)len * std::log((double)len + (double)K * (double)p->alpha);
     }
-    // docs longest first for the theta rebuild's warps: a counting sort on
-    // the length (below 65536), stable in doc id
-    std::vector<int32_t> doc_order((size_t)D);
-    {
-        std::vector<int32_t> start(65537, 0);
-        for (int32_t d = 0; d < D; ++d) start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d])) + 1]++;
-        for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
-        for (int32_t d = 0; d < D; ++d)
-            doc_order[(size_t)start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d]))]++] = d;
-    }
     // grids
     const int sms = num_sms(ctx->device);
     int sbps = sample_blocks_per_sm(K, gl, sb);
@@ -816,12 +806,24 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
             arena.use(ctx->d_block + from, size - from);
     };
 
+    mark("host layout, block");
     // corpus upload
     CKB(cudaMemcpyAsync(ctx->d_word_ptr, c->word_ptr, sizeof(int64_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_doc_ptr, c->doc_ptr, sizeof(int64_t) * ((size_t)D + 1), cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_doc_ids, c->doc_ids, sizeof(int32_t) * (size_t)N, cudaMemcpyHostToDevice, s));
     CKB(cudaMemsetAsync(ctx->d_error, 0, 64 * sizeof(int32_t), s));
-    // the rest of the host layout goes up while the corpus does
+    // docs longest first for the theta rebuild's warps: a counting sort on
+    // the length (below 65536), stable in doc id, on the host while the
+    // corpus goes up
+    std::vector<int32_t> doc_order((size_t)D);
+    {
+        std::vector<int32_t> start(65537, 0);
+        for (int32_t d = 0; d < D; ++d) start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d])) + 1]++;
+        for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+        for (int32_t d = 0; d < D; ++d)
+            doc_order[(size_t)start[(size_t)(65535 - (c->doc_ptr[d + 1] - c->doc_ptr[d]))]++] = d;
+    }
+    // the rest of the host layout goes up behind the corpus
     CKB(cudaMemcpyAsync(ctx->d_rows, rows.data(), sizeof(int2) * (size_t)D, cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_doc_order, doc_order.data(), sizeof(int32_t) * (size_t)D, cudaMemcpyHostToDevice, s));
     CKB(cudaMemcpyAsync(ctx->d_items, items.data(), sizeof(culda_item) * items.size(), cudaMemcpyHostToDevice, s));

@@ -605,9 +605,10 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
 
         double ll = 0.0;
         const int sg_end = item.seg_begin + item.seg_count;
-        // chunks of a quarter of the item's segments (8 to 32), so the four
-        // warps share small items too
-        const int cs = min(kFlatSegs, max(8, (item.seg_count + kFlatWarps - 1) / kFlatWarps));
+        // chunks of a quarter of the item's segments (at most 32), so the four
+        // warps share small items too (on the uneven 118M-token workload a
+        // floor of 1 segment beat floors of 2, 4, 8 and 16)
+        const int cs = min(kFlatSegs, max(1, (item.seg_count + kFlatWarps - 1) / kFlatWarps));
         for (;;) {
             int ch = 0;
             if (lane == 0) ch = atomicAdd(&s_chunk, 1);

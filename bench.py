@@ -404,7 +404,9 @@ def run_ours(args, world, rank, local, pg):
         m2 = cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed + rank, device=local,
                     group_lanes=args.group_lanes, item_tokens=args.item_tokens, sample_blocks=args.sample_blocks,
                     flags=run_flags(args))
+        t_created = time.perf_counter()
         lls = [s["loglik"] for s in m2.iterate(args.steps)]
+        t_iterated = time.perf_counter()
         st = cb.lib().culda_get_topics(m2._ctx, C.cast(z_host.data_ptr(), C.POINTER(C.c_uint16)))
         cuda_sync()
         t1 = time.perf_counter()
@@ -419,6 +421,8 @@ def run_ours(args, world, rank, local, pg):
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                "seconds": round(e2e_sec, 4), "includes": "culda_create (upload, doc index sort, initial counts, "
                "graph capture) + K iterations each reading its log-likelihood back + final topic download",
+               "seconds_by_part": {"create": round(t_created - t0, 4), "iterations": round(t_iterated - t_created, 4),
+                                   "download": round(t1 - t_iterated, 4)},
                "loglik_last": lls[-1] if lls else None}
 
     # ---- CPU baseline (rank 0, one GPU only): the OpenMP port of the same rule

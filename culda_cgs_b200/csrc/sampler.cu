@@ -6,10 +6,15 @@
 // snapshot topics (no dense V x K phi in HBM), phihat = (n_wk + beta) /
 // (n_k + V beta) is formed in FP32 at shared-memory offset 0, and the
 // alpha*phihat prefix of the dense bucket is scanned.  The item's tokens come
-// in segments (runs of one doc, at most 32 tokens): a group of G lanes walks
-// the doc's theta row once per segment with 32-byte loads (4 entries per lane
-// per step), keeping the running sum after every step in shared memory, and
-// then draws each token of the segment with its own Philox uniform.
+// in segments (runs of one doc, at most 32 tokens) that share one walk of the
+// doc's theta row and differ only in their Philox uniforms.  Two samplers do
+// the walks and draws:
+//   sample_flat_kernel (the default): a warp splits the rows of a batch of
+//     segments evenly over 8 groups of 4 lanes, builds every row's prefix
+//     sums in shared memory, and each lane then draws its own tokens;
+//   sample_kernel<G>: a group of G lanes walks one row with 32-byte loads
+//     (8 entries per lane per step), keeps the running sum after every step
+//     in shared memory, and draws the segment's tokens one after another.
 //
 // A theta entry is one 32-bit word: the count in the low 16 bits and 4 * topic
 // (the byte offset of the topic's phihat) in the high 16 bits.  The product

@@ -319,7 +319,12 @@ int pick_group_lanes(int requested, int k) {
     return requested == 0 ? kFlatLanes : 0;  // 0: not a variant
 }
 
-int pick_sample_blocks(int requested) { return requested != 0 ? requested : kSampleBlocksDefault; }
+// the flat walk's default is the 48-register build (10 CTAs per SM), the
+// group samplers' the 64-register one
+int pick_sample_blocks(int requested, int group_lanes) {
+    if (requested != 0) return requested;
+    return group_lanes == kFlatLanes ? kSampleBlocksHigh : kSampleBlocksDefault;
+}
 
 
 }  // namespace
@@ -563,7 +568,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: CULDA_FLAG_AUTOTUNE needs group_lanes = sample_blocks = 0");
     const int gl = pick_group_lanes(p->group_lanes, p->k);
     if (gl == 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: group_lanes=%d", p->group_lanes);
-    const int sb = pick_sample_blocks(p->sample_blocks);
+    const int sb = pick_sample_blocks(p->sample_blocks, gl);
     if (!sample_variant_exists(gl, sb))
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: no sampler for group_lanes=%d sample_blocks=%d", gl,
                     p->sample_blocks);

@@ -571,10 +571,11 @@ extern "C" int culda_sample(const culda_sample_args *a, void *d_workspace, size_
     p.error = a->error ? a->error : counter + 1;
     int dev = 0;
     cudaGetDevice(&dev);
-    int bps = sample_blocks_per_sm(a->k, a->group_lanes, kSampleBlocksDefault);
+    const int blocks = a->group_lanes == kFlatLanes ? kSampleBlocksHigh : kSampleBlocksDefault;
+    int bps = sample_blocks_per_sm(a->k, a->group_lanes, blocks);
     if (bps <= 0) bps = 1;
     const int grid = std::max(1, std::min(a->num_items, num_sms(dev) * bps));
-    rc = cuda_status(launch_sample(p, a->group_lanes, kSampleBlocksDefault, grid, s));
+    rc = cuda_status(launch_sample(p, a->group_lanes, blocks, grid, s));
     if (rc) return rc;
     DevStats *st = (DevStats *)(counter + 8);
     rc = cuda_status(launch_finalize_ll(item_ll, a->num_items, st, nullptr, s));

@@ -541,8 +541,7 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
     extern __shared__ float smem[];
     const int K = p.k, KP = p.kmask + 1, B = flat_unit_budget(K);
     float *ph = smem;               // [KP] phihat of the current word (zero past K), at offset 0
-    float *inv = smem + KP;         // [K]  1 / (n_k + V beta)
-    float *qc = inv + K;            // [K]  dense-bucket prefix (the word histogram before that)
+    float *qc = smem + KP;          // [K]  dense-bucket prefix (the word histogram before that)
     int *hist = reinterpret_cast<int *>(qc);
     __shared__ int s_item, s_chunk;
     __shared__ float s_warp[kSampleThreads / 32];
@@ -560,7 +559,6 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
     float *m_lg = m_S + kFlatSegs;                               // [n] log(S + Q)
     const uint32_t iter = p.iteration_ptr ? *p.iteration_ptr : p.iteration;
 
-    for (int j = tid; j < K; j += blockDim.x) inv[j] = 1.0f / ((float)p.nk[j] + p.vbeta);
     for (int j = K + tid; j < KP; j += blockDim.x) ph[j] = 0.f;
 
     for (;;) {
@@ -602,7 +600,11 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
         } else {
             src = p.hot_phi + (size_t)item.hot * K;
         }
-        for (int j = tid; j < K; j += blockDim.x) ph[j] = ((float)src[j] + p.beta) * inv[j];
+        // 1 / (n_k + V beta) is formed per item (the same operations, so the
+        // same bits, as a table would hold): without the table's 4 KB the
+        // 48-register build fits 10 CTAs per SM
+        for (int j = tid; j < K; j += blockDim.x)
+            ph[j] = ((float)src[j] + p.beta) * (1.0f / ((float)__ldg(p.nk + j) + p.vbeta));
         __syncthreads();
         dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
         __syncthreads();
@@ -809,8 +811,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
 }
 
 size_t sample_smem_bytes(int k, int group_lanes) {
-    if (group_lanes == kFlatLanes)  // ph[pow2(K)] + inv[K] + qc[K] + per warp: unit prefixes and segment data
-        return ((size_t)2 * k + (size_t)pow2_ceil(k) + (size_t)kFlatWarps * flat_unit_budget(k) +
+    if (group_lanes == kFlatLanes)  // ph[pow2(K)] + qc[K] + per warp: unit prefixes and segment data
+        return ((size_t)k + (size_t)pow2_ceil(k) + (size_t)kFlatWarps * flat_unit_budget(k) +
                 (size_t)kFlatWarps * kFlatMeta) *
                sizeof(float);
     // ph[pow2(K)] + inv[K] + qc[K] + the per-group running sums

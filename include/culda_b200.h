@@ -179,8 +179,9 @@ typedef struct culda_params {
                              walk, else 1,2,4,8,16,32 lanes per token */
     int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto, at most 65535 */
     int32_t flags;        /* CULDA_FLAG_* */
-    int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (8),
-                              8 (<= 64 registers), or 10 (<= 48 registers; the flat walk and
+    int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (10
+                              for the flat walk, 8 for the group samplers), 8 (<= 64
+                              registers), or 10 (<= 48 registers; the flat walk and
                               group_lanes 4, 8, 16) */
 } culda_params;
 

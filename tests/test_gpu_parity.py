@@ -89,7 +89,7 @@ def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens, 
     seed = 1234
     with cb.LDA(c, k, 50.0 / 1024, 0.01, seed=seed, group_lanes=g, item_tokens=item_tokens,
                 sample_blocks=blocks) as m:
-        assert m.info()["sample_blocks"] == (blocks or 8)
+        assert m.info()["sample_blocks"] == (blocks or (10 if g == -1 else 8))
         z0 = m.topics()
         assert np.array_equal(z0, O.init_topics(c.num_tokens, k, seed))
         s0 = assert_counts_exact(m, c)

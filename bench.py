@@ -320,6 +320,17 @@ def measure_foldin(args, device) -> dict:
     return out
 
 
+def common_config(wl, num_tokens: int, num_docs: int, num_words: int, seed: int, world: int) -> dict:
+    """The `config` object both arms print: the workload and its sizes only,
+    so the two lines compare key for key."""
+    return {"workload": wl.name, "num_tokens": int(num_tokens), "num_docs": int(num_docs),
+            "num_words": int(num_words), "k": wl.k, "alpha": wl.alpha, "beta": wl.beta, "seed": seed,
+            "l2": (f"inputs larger than L2 (doc ids, doc-reverse index, topics, uniforms and theta: at least "
+                   f"{20 * num_tokens / 1e9:.2f} GB against 126 MB), no flush"
+                   if 20 * num_tokens > 126e6 else "inputs smaller than L2 (small workload, not a headline line)"),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
 # ------------------------------------------------------------------- ours
 def run_ours(args, world, rank, local, pg):
     import ctypes as C
@@ -421,8 +432,8 @@ def run_ours(args, world, rank, local, pg):
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                "seconds": round(e2e_sec, 4), "includes": "culda_create (upload, doc index sort, initial counts, "
                "graph capture) + K iterations each reading its log-likelihood back + final topic download",
-               "seconds_by_part": {"create": round(t_created - t0, 4), "iterations": round(t_iterated - t_created, 4),
-                                   "download": round(t1 - t_iterated, 4)},
+               "create_seconds": round(t_created - t0, 4), "iterations_seconds": round(t_iterated - t_created, 4),
+               "download_seconds": round(t1 - t_iterated, 4),
                "loglik_last": lls[-1] if lls else None}
 
     # ---- CPU baseline (rank 0, one GPU only): the OpenMP port of the same rule
@@ -459,14 +470,11 @@ def run_ours(args, world, rank, local, pg):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * max_seconds / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded generator, shapes of the workload)",
-        "config": {"workload": wl.name, "num_tokens": N, "num_docs": corpus.num_docs, "num_words": corpus.num_words,
-                   "k": wl.k, "alpha": wl.alpha, "beta": wl.beta, "seed": args.seed,
-                   "group_lanes": info["group_lanes"], "sample_blocks": info["sample_blocks"],
-                   "token_order": "input" if args.no_reorder else "by doc length inside each word",
-                   "autotuned": bool(info["tuned"]),
-                   "items": info["num_items"], "hot_words": info["num_hot"],
-                   "l2": f"inputs larger than L2 (resident set {info['device_bytes'] / 1e9:.2f} GB > 126 MB)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": common_config(wl, N, corpus.num_docs, corpus.num_words, args.seed, world),
+        "variant": {"group_lanes": info["group_lanes"], "sample_blocks": info["sample_blocks"],
+                    "token_order": "input" if args.no_reorder else "by doc length inside each word",
+                    "autotuned": bool(info["tuned"]), "items": info["num_items"], "hot_words": info["num_hot"],
+                    "resident_gb": round(info["device_bytes"] / 1e9, 3)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         "learned": learned, "foldin": foldin,
         "loglik": [round(s["loglik"], 8) for s in stats],
@@ -478,23 +486,43 @@ def run_ours(args, world, rank, local, pg):
 ITER_RE = re.compile(r"Iteration\s+(\d+):\s+([\d.]+) sec,\s+([\d.]+) sec, logLikelyhood = ([-\d.naninf]+),\s+([\d.]+) M")
 
 
+def repo_library_mapped() -> bool:
+    """True when this process has mapped the repository's own library."""
+    try:
+        return "libculda_b200.so" in Path("/proc/self/maps").read_text()
+    except OSError:
+        return False
+
+
+def gencorpus_command(gen, prefix: str) -> list[str]:
+    """culda_cgs_b200/bin/gencorpus arguments for a GenConfig: the corpus is
+    generated and written by that host program, so the reference arm's own
+    process never loads the repository's library."""
+    law = {0: "poisson", 1: "lognormal", 2: "pareto"}[gen.len_law]
+    return [str(ROOT / "culda_cgs_b200" / "bin" / "gencorpus"), "-words", str(gen.num_words),
+            "-topics", str(gen.num_topics), "-docs", str(gen.num_docs), "-law", law, "-a", repr(float(gen.len_a)),
+            "-b", repr(float(gen.len_b)), "-min", str(gen.len_min), "-max", str(gen.len_max),
+            "-zipf", repr(float(gen.zipf_s)), "-wconc", repr(float(gen.word_conc)),
+            "-dconc", repr(float(gen.doc_conc)), "-seed", str(gen.seed), "-threads", str(gen.threads), "-o", prefix]
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
     binary = ROOT / "oracle" / "_ref" / "culda"
     if not binary.exists():
         return {"impl": "reference", "unavailable": "oracle/_ref/culda was not built (reference sources absent)"}
-    import culda_cgs_b200 as cb
-    from culda_cgs_b200.configs import WORKLOADS
-
     wl = workload(args, args.seed)
     if wl.k != 1024:
         return {"impl": "reference", "unavailable": "the reference kernel supports only K=1024"}
-    corpus = cb.Corpus.generate(wl.gen)
-    N = corpus.num_tokens
     tmp = Path(tempfile.mkdtemp(prefix="culda_ref_"))
     try:
-        corpus.write(str(tmp / "corpus"))
+        g = subprocess.run(gencorpus_command(wl.gen, str(tmp / "corpus")), capture_output=True, text=True,
+                           timeout=600)
+        if g.returncode != 0:
+            return {"impl": "reference", "unavailable": f"corpus generation failed: {g.stderr.strip()[-200:]}"}
+        sizes = json.loads(g.stdout.strip().splitlines()[-1])
+        N = int(sizes["num_tokens"])
         iters = args.warmup + args.steps
         cmd = [str(binary), "-g", "1", "-c", "1", "-k", str(wl.k), "-t", str(iters), "-s", "1",
                "-a", repr(float(wl.alpha)), "-b", repr(float(wl.beta)), "-i", str(tmp / "corpus")]
@@ -519,10 +547,12 @@ def run_reference(args, world, rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * sum(stamps) / len(stamps), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp16 phiHead / fp32 sums",
             "data": "synthetic (seeded generator, shapes of the workload)",
-            "config": {"workload": wl.name, "num_tokens": N, "num_docs": corpus.num_docs,
-                       "num_words": corpus.num_words, "k": wl.k, "alpha": wl.alpha, "beta": wl.beta,
-                       "seed": args.seed, "parallelism": "single GPU",
-                       "timing": "the reference's own per-iteration host clock (SingleChunkSingleGPU.h:72-127)"},
+            "config": common_config(wl, N, sizes["num_docs"], sizes["num_words"], args.seed, 1),
+            "timing": "the reference's own per-iteration host clock (SingleChunkSingleGPU.h:72-127)",
+            "binary": "oracle/_ref/culda: the reference's src_culda compiled unmodified for sm_100a "
+                      "(oracle/build_oracle.py, compatibility header only)",
+            "corpus_writer": "culda_cgs_b200/bin/gencorpus in its own process",
+            "repo_library_mapped": repo_library_mapped(),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": f"iterations {args.warmup + 1}-{iters} of the reference's CUDA build "
                                        "(oracle/_ref/culda, sm_100a) on one B200, driven by one host thread"},

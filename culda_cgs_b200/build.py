@@ -6,6 +6,7 @@ objects and binaries travel with the source tree:
     culda_cgs_b200/libculda_b200.so   CUDA kernels + C ABI (include/culda_b200.h)
     culda_cgs_b200/bin/culda          C++ host with the reference's CLI
     culda_cgs_b200/bin/format         C++ host with the reference's preprocessing tool
+    culda_cgs_b200/bin/gencorpus      C++ host writing a seeded synthetic corpus in the src_format files
     oracle/liboracle.so               host FP64 oracle + OpenMP CPU baseline (tests/bench only)
     oracle/_ref/...                   the reference's own build (only where its sources exist)
 """
@@ -23,6 +24,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libculda_b200.so"
 CLI = PKG / "bin" / "culda"
 FORMAT_CLI = PKG / "bin" / "format"
+GEN_CLI = PKG / "bin" / "gencorpus"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # portable host ISA: the library is built here and run on the GPU hosts
 HOST_ARCH = "-march=x86-64-v2"
@@ -94,10 +96,15 @@ def build_format_cli(verbose: bool = False, force: bool = False) -> Path:
     return _build_host_tool(CSRC / "cli" / "format_main.cpp", FORMAT_CLI, verbose, force)
 
 
+def build_gencorpus_cli(verbose: bool = False, force: bool = False) -> Path:
+    return _build_host_tool(CSRC / "cli" / "gencorpus_main.cpp", GEN_CLI, verbose, force)
+
+
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_library(verbose, force)
     build_cli(verbose, force)
     build_format_cli(verbose, force)
+    build_gencorpus_cli(verbose, force)
     sys.path.insert(0, str(ROOT))
     from oracle import build_oracle  # the checker is built beside the product, never linked into it
 

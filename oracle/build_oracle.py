@@ -17,7 +17,9 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 LIB = HERE / "liboracle.so"
 REF_OUT = HERE / "_ref"
-REFERENCE = Path(os.environ.get("CULDA_REFERENCE_SRC", "/root/reference"))
+# the reference's source tree: CULDA_REFERENCE_SRC, else a `reference` directory
+# beside this repository
+REFERENCE = Path(os.environ.get("CULDA_REFERENCE_SRC", str(ROOT.parent / "reference")))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -78,6 +78,7 @@ double oracle_uniform(uint32_t x) { return (double)((((x >> 9) << 1) | 1u)) * 0x
 /* Initial topics: z_t = floor(x0 * K / 2^32) with x0 = Philox(seed, {t, 0, 1}).
  * (The reference draws rand() % K after srand(time(NULL)), doc_chunk.cpp:259-264.) */
 void oracle_init_topics(int64_t n, int32_t k, uint64_t seed, uint16_t *z) {
+#pragma omp parallel for schedule(static)
     for (int64_t t = 0; t < n; ++t) {
         uint32_t x = philox_word0(seed, (uint64_t)t, 0u, 1u);
         z[t] = (uint16_t)(((uint64_t)x * (uint64_t)k) >> 32);
@@ -111,14 +112,13 @@ int64_t oracle_theta_layout(int32_t num_docs, int32_t k, const int64_t *doc_ptr,
 void oracle_phi_counts(int32_t num_words, int32_t k, const int64_t *word_ptr, const uint16_t *z, int32_t *phi,
                        int32_t *nk) {
     std::memset(nk, 0, sizeof(int32_t) * (size_t)k);
+#pragma omp parallel for schedule(dynamic, 64)
     for (int32_t w = 0; w < num_words; ++w) {
         int32_t *row = phi + (size_t)w * k;
         std::memset(row, 0, sizeof(int32_t) * (size_t)k);
-        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) {
-            row[z[t]]++;
-            nk[z[t]]++;
-        }
+        for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) row[z[t]]++;
     }
+    for (int64_t t = word_ptr[0]; t < word_ptr[num_words]; ++t) nk[z[t]]++;
 }
 
 /* IEEE binary16 round-to-nearest-even of a float, from the format definition. */
@@ -193,7 +193,10 @@ void oracle_phi_head_f16(int32_t num_words, int32_t k, float beta, const int32_t
 void oracle_theta_csr(int32_t num_docs, int32_t k, const int64_t *doc_ptr, const int32_t *doc_tok,
                       const uint16_t *z, const int32_t *max_ia, int16_t *theta_a, int16_t *theta_ja,
                       int32_t *cur_ia) {
+#pragma omp parallel
+    {
     std::vector<int32_t> dense((size_t)k);
+#pragma omp for schedule(dynamic, 256)
     for (int32_t d = 0; d < num_docs; ++d) {
         std::fill(dense.begin(), dense.end(), 0);
         for (int64_t i = doc_ptr[d]; i < doc_ptr[d + 1]; ++i) dense[z[doc_tok[i]]]++;
@@ -209,6 +212,7 @@ void oracle_theta_csr(int32_t num_docs, int32_t k, const int64_t *doc_ptr, const
                 ++nnz;
             }
         cur_ia[d] = start + (nnz + 31) / 32 * 32;
+    }
     }
 }
 
@@ -389,6 +393,163 @@ void oracle_sample_fixed_fp64(int32_t num_docs, int32_t num_words, int32_t k, fl
     if (loglik_terms) {
         loglik_terms[0] = s_log + c_log;
         loglik_terms[1] = s_doc + c_doc;
+    }
+}
+
+/*
+ * The same FP64 rule as oracle_sample_fixed_fp64 (lda_train_kernel.cu:65-259,
+ * per-token log term :258) for a selection of tokens:
+ * sel holds ascending word-major token indices (NULL = every token), z_out,
+ * margin and ll_tok (each may be NULL) are indexed like sel, and ll_tok[i] is
+ * the token's log term log(S+Q) - log(L_d + K*alpha).  Each word's phi row is
+ * counted from z on the fly (no V x K table), so corpora of any vocabulary
+ * fit; the work runs on all host threads in runs of at most 32768 selected
+ * tokens of one word (the rows of words cut into several runs are counted
+ * once, first).  ll_terms receives sum log(S+Q) and sum log(L_d + K*alpha)
+ * over the selection, each run's Neumaier sum added in run order.
+ */
+void oracle_sample_tokens_fp64(int32_t num_docs, int32_t num_words, int32_t k, float alpha_f, float beta_f,
+                               const int64_t *word_ptr, const int32_t *doc_ids, const int64_t *doc_ptr,
+                               const uint16_t *z, const int32_t *nk, const int16_t *theta_a,
+                               const int16_t *theta_ja, const int32_t *max_ia, const int32_t *cur_ia, uint64_t seed,
+                               uint32_t iteration, int64_t n_sel, const int64_t *sel, uint16_t *z_out,
+                               double *margin, double *ll_tok, double *ll_terms) {
+    (void)num_docs;
+    const double alpha = alpha_f, beta = beta_f;
+    const double vbeta = (double)num_words * beta;
+    const int64_t total_tokens = word_ptr[num_words] - word_ptr[0];
+    if (!sel) n_sel = total_tokens;
+    auto token_at = [&](int64_t i) -> int64_t { return sel ? sel[i] : word_ptr[0] + i; };
+    auto word_of = [&](int64_t t) -> int32_t {
+        return (int32_t)(std::upper_bound(word_ptr, word_ptr + num_words + 1, t) - word_ptr - 1);
+    };
+    // runs: [begin, end) of the selection, all of one word, at most kRun long
+    const int64_t kRun = 32768;
+    struct Run { int64_t begin, end; int32_t word, shared_row; };
+    std::vector<Run> runs;
+    std::vector<int32_t> shared_words;
+    for (int64_t i = 0; i < n_sel;) {
+        const int32_t w = word_of(token_at(i));
+        int64_t j = i;
+        if (sel) {
+            while (j < n_sel && sel[j] < word_ptr[w + 1]) ++j;
+        } else {
+            j = word_ptr[w + 1] - word_ptr[0];
+        }
+        const bool split = (j - i) > kRun;
+        if (split) shared_words.push_back(w);
+        for (int64_t b = i; b < j; b += kRun)
+            runs.push_back({b, std::min(j, b + kRun), w, split ? (int32_t)shared_words.size() - 1 : -1});
+        i = j;
+    }
+    std::vector<double> den((size_t)k);
+    for (int32_t j = 0; j < k; ++j) den[j] = (double)nk[j] + vbeta;
+    // phi rows of the words cut into several runs
+    std::vector<double> shared((size_t)shared_words.size() * k);
+#pragma omp parallel
+    {
+        std::vector<int32_t> hist((size_t)k);
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t r = 0; r < (int64_t)shared_words.size(); ++r) {
+            const int32_t w = shared_words[r];
+            std::fill(hist.begin(), hist.end(), 0);
+            for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) hist[z[t]]++;
+            for (int32_t j = 0; j < k; ++j) shared[(size_t)r * k + j] = ((double)hist[j] + beta) / den[j];
+        }
+    }
+    std::vector<double> run_log(runs.size() * 2), run_doc(runs.size() * 2);
+#pragma omp parallel
+    {
+        std::vector<int32_t> hist((size_t)k);
+        std::vector<double> own((size_t)k);
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t r = 0; r < (int64_t)runs.size(); ++r) {
+            const Run &run = runs[r];
+            const int32_t w = run.word;
+            const double *ph;
+            if (run.shared_row >= 0) {
+                ph = &shared[(size_t)run.shared_row * k];
+            } else {
+                std::fill(hist.begin(), hist.end(), 0);
+                for (int64_t t = word_ptr[w]; t < word_ptr[w + 1]; ++t) hist[z[t]]++;
+                for (int32_t j = 0; j < k; ++j) own[j] = ((double)hist[j] + beta) / den[j];
+                ph = own.data();
+            }
+            double q = 0;
+            for (int32_t j = 0; j < k; ++j) q += alpha * ph[j];
+            double s_log = 0, c_log = 0, s_doc = 0, c_doc = 0;
+            for (int64_t i = run.begin; i < run.end; ++i) {
+                const int64_t t = token_at(i);
+                const int32_t d = doc_ids[t];
+                const int32_t rs = max_ia[d], re = cur_ia[d];
+                double s = 0;
+                for (int32_t e = rs; e < re; ++e)
+                    if (theta_a[e] != 0) s += (double)(uint16_t)theta_a[e] * ph[(uint16_t)theta_ja[e]];
+                const double tot = s + q;
+                const double target = oracle_uniform(philox_word0(seed, (uint64_t)t, iteration, 0u)) * tot;
+                int32_t pick = -1;
+                double lo = 0, hi = tot;
+                if (target < s) {
+                    double cum = 0;
+                    int32_t last = -1;
+                    for (int32_t e = rs; e < re; ++e) {
+                        if (theta_a[e] == 0) continue;
+                        const double nxt = cum + (double)(uint16_t)theta_a[e] * ph[(uint16_t)theta_ja[e]];
+                        last = e;
+                        if (nxt > target) {
+                            pick = (uint16_t)theta_ja[e];
+                            lo = cum;
+                            hi = nxt;
+                            break;
+                        }
+                        cum = nxt;
+                    }
+                    if (pick < 0) {
+                        pick = (uint16_t)theta_ja[last];
+                        lo = cum;
+                        hi = s;
+                    }
+                } else {
+                    double cum = s;
+                    for (int32_t j = 0; j < k; ++j) {
+                        const double nxt = cum + alpha * ph[j];
+                        if (nxt > target) {
+                            pick = j;
+                            lo = cum;
+                            hi = nxt;
+                            break;
+                        }
+                        cum = nxt;
+                    }
+                    if (pick < 0) {
+                        pick = k - 1;
+                        lo = cum;
+                        hi = tot;
+                    }
+                }
+                const double dl = std::log((double)(doc_ptr[d + 1] - doc_ptr[d]) + (double)k * alpha);
+                if (z_out) z_out[i] = (uint16_t)pick;
+                if (margin) margin[i] = std::min(target - lo, hi - target) / tot;
+                if (ll_tok) ll_tok[i] = std::log(tot) - dl;
+                neumaier_add(s_log, c_log, std::log(tot));
+                neumaier_add(s_doc, c_doc, dl);
+            }
+            run_log[2 * r] = s_log;
+            run_log[2 * r + 1] = c_log;
+            run_doc[2 * r] = s_doc;
+            run_doc[2 * r + 1] = c_doc;
+        }
+    }
+    if (ll_terms) {
+        double s1 = 0, c1 = 0, s2 = 0, c2 = 0;
+        for (size_t r = 0; r < runs.size(); ++r) {
+            neumaier_add(s1, c1, run_log[2 * r]);
+            neumaier_add(s1, c1, run_log[2 * r + 1]);
+            neumaier_add(s2, c2, run_doc[2 * r]);
+            neumaier_add(s2, c2, run_doc[2 * r + 1]);
+        }
+        ll_terms[0] = s1 + c1;
+        ll_terms[1] = s2 + c2;
     }
 }
 

@@ -248,6 +248,60 @@ class Snapshot:
         return vp, vt
 
 
+@dataclass
+class RowSnapshot:
+    """n_k and the theta CSR of one topic assignment, without the V x K phi
+    table (which does not fit at a million words and K = 4096): the rows the
+    samplers read.  Built by the oracle from scratch."""
+    num_docs: int
+    num_words: int
+    k: int
+    alpha: float
+    beta: float
+    word_ptr: np.ndarray
+    doc_ids: np.ndarray
+    doc_ptr: np.ndarray
+    z: np.ndarray
+    nk: np.ndarray
+    theta_a: np.ndarray
+    theta_ja: np.ndarray
+    max_ia: np.ndarray
+    cur_ia: np.ndarray
+
+    @classmethod
+    def build(cls, word_ptr, doc_ids, doc_ptr, z, k, alpha, beta) -> "RowSnapshot":
+        word_ptr, doc_ids, doc_ptr = _c(word_ptr, np.int64), _c(doc_ids, np.int32), _c(doc_ptr, np.int64)
+        z = _c(z, np.uint16)
+        d = len(doc_ptr) - 1
+        doc_tok = doc_rev(d, doc_ids, doc_ptr)
+        max_ia = theta_layout(d, k, doc_ptr)
+        a, ja, cur = theta_csr(d, k, doc_ptr, doc_tok, z, max_ia)
+        del doc_tok
+        nk = np.bincount(z, minlength=k).astype(np.int32)
+        return cls(d, len(word_ptr) - 1, k, float(np.float32(alpha)), float(np.float32(beta)), word_ptr, doc_ids,
+                   doc_ptr, z, nk, a, ja, max_ia, cur)
+
+    def sample_tokens(self, seed: int, iteration: int, sel=None, per_token_ll: bool = True):
+        """(z_new, margin, ll_tok, (sum log(S+Q), sum doc term)) for the tokens
+        `sel` (ascending word-major indices; None = all), one FP64 draw each
+        (oracle_sample_tokens_fp64); ll_tok is None unless per_token_ll."""
+        sel_arr = None if sel is None else _c(sel, np.int64)
+        n = len(self.z) if sel_arr is None else len(sel_arr)
+        if sel_arr is not None and n > 1:
+            assert (np.diff(sel_arr) > 0).all(), "selection must be ascending"
+        z_out = np.empty(n, dtype=np.uint16)
+        margin = np.empty(n, dtype=np.float64)
+        ll_tok = np.empty(n, dtype=np.float64) if per_token_ll else None
+        terms = np.zeros(2, dtype=np.float64)
+        lib().oracle_sample_tokens_fp64(
+            C.c_int32(self.num_docs), C.c_int32(self.num_words), C.c_int32(self.k), C.c_float(self.alpha),
+            C.c_float(self.beta), _p(self.word_ptr), _p(self.doc_ids), _p(self.doc_ptr), _p(self.z), _p(self.nk),
+            _p(self.theta_a), _p(self.theta_ja), _p(self.max_ia), _p(self.cur_ia), C.c_uint64(seed),
+            C.c_uint32(iteration), C.c_int64(n), _p(sel_arr) if sel_arr is not None else None, _p(z_out), _p(margin),
+            _p(ll_tok) if ll_tok is not None else None, _p(terms))
+        return z_out, margin, ll_tok, (float(terms[0]), float(terms[1]))
+
+
 def loglik_reference(snapshot: "Snapshot", num_tokens: int, slot_word, slot_range, phi_head_f16_table) -> float:
     """The log-likelihood the reference prints (oracle_loglik_reference)."""
     s = snapshot

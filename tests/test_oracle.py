@@ -160,3 +160,42 @@ def test_half_conversion():
     xs = np.float32(np.random.default_rng(0).lognormal(-8, 4, 20000))
     assert np.array_equal(np.array([O.float_to_half(float(x)) for x in xs], dtype=np.uint16),
                           xs.astype(np.float16).view(np.uint16))
+
+
+def test_token_selection_sampler_equals_the_full_oracle(tiny):
+    """oracle_sample_tokens_fp64 (rows counted on the fly, all host threads)
+    gives the draws, margins and log-likelihood of the whole-corpus oracle,
+    for every token and for any ascending selection."""
+    c, s = tiny
+    r = O.RowSnapshot.build(c.word_ptr, c.doc_ids, c.doc_ptr, s.z, s.k, TINY.alpha, TINY.beta)
+    assert np.array_equal(r.nk, s.nk) and np.array_equal(r.theta_a, s.theta_a) and np.array_equal(r.cur_ia, s.cur_ia)
+    z_all, m_all, ll_all = s.sample(5, 3)
+    z, m, ll_tok, (t_log, t_doc) = r.sample_tokens(5, 3)
+    assert np.array_equal(z, z_all) and np.array_equal(m, m_all)
+    assert (t_log - t_doc) / len(z) == pytest.approx(ll_all, rel=1e-12)
+    assert ll_tok.sum() == pytest.approx(t_log - t_doc, rel=1e-12)
+    sel = np.sort(np.random.default_rng(0).choice(len(s.z), 700, replace=False))
+    z2, m2, ll2, _ = r.sample_tokens(5, 3, sel)
+    assert np.array_equal(z2, z_all[sel]) and np.array_equal(m2, m_all[sel]) and np.allclose(ll2, ll_tok[sel])
+
+
+def test_token_selection_sampler_splits_a_hot_word_into_runs():
+    """A word of 70,000 tokens is cut into runs of 32,768 that share one
+    counted row: the draws equal the whole-corpus oracle's."""
+    rng = np.random.default_rng(3)
+    D, K = 40, 64
+    hot = np.sort(rng.integers(0, D, 70_000)).astype(np.int32)
+    cold = [np.sort(rng.integers(0, D, n)).astype(np.int32) for n in (5, 300, 1)]
+    doc_ids = np.concatenate([hot, *cold])
+    word_ptr = np.concatenate([[0], np.cumsum([len(hot)] + [len(x) for x in cold])]).astype(np.int64)
+    doc_ptr = np.concatenate([[0], np.cumsum(np.bincount(doc_ids, minlength=D))]).astype(np.int64)
+    z = O.init_topics(len(doc_ids), K, 9)
+    s = O.Snapshot.build(word_ptr, doc_ids, doc_ptr, z, K, 0.1, 0.01)
+    r = O.RowSnapshot.build(word_ptr, doc_ids, doc_ptr, z, K, 0.1, 0.01)
+    z_all, m_all, ll_all = s.sample(7, 2)
+    zr, mr, _, (t_log, t_doc) = r.sample_tokens(7, 2)
+    assert np.array_equal(zr, z_all) and np.array_equal(mr, m_all)
+    assert (t_log - t_doc) / len(z) == pytest.approx(ll_all, rel=1e-12)
+    sel = np.r_[np.arange(0, 70_000, 7), 70_000 + np.arange(306)]
+    zs, ms, _, _ = r.sample_tokens(7, 2, sel)
+    assert np.array_equal(zs, z_all[sel]) and np.array_equal(ms, m_all[sel])

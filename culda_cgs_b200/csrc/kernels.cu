@@ -504,7 +504,7 @@ extern "C" int culda_sample(const culda_sample_args *a, void *d_workspace, size_
         !a->doc_ids || !a->topics_in || !a->topics_out || a->topics_in == a->topics_out || !a->theta ||
         !a->theta_rows || !a->nk || !a->items || a->num_items <= 0 || !a->seg_start || a->num_segs <= 0 ||
         !a->loglik_sum || !d_workspace ||
-        (a->num_hot > 0 && (!a->hot_items || a->num_hot_items <= 0)) || a->theta_capacity <= 0 ||
+        a->num_hot < 0 || (a->num_hot > 0 && (!a->hot_items || a->num_hot_items <= 0)) || a->theta_capacity <= 0 ||
         workspace_bytes < culda_sample_workspace(a->k, a->num_items, a->num_hot) ||
         (a->group_lanes != kFlatLanes && a->group_lanes != 1 && a->group_lanes != 2 && a->group_lanes != 4 &&
          a->group_lanes != 8 && a->group_lanes != 16 && a->group_lanes != 32) ||

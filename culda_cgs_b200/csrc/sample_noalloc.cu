@@ -1,14 +1,14 @@
 // sample_noalloc.cu — culda_sample_noalloc: the kernel-level sampler with its
 // scratch memory in a fixed device array instead of a caller workspace.
 //
-// Who needs it: an application that owns all device memory through its own
-// pool allocator and does not let libraries call cudaMalloc, or a
-// latency-sensitive loop that cannot pay the device-wide synchronisation an
-// allocation implies, cannot hand culda_sample a workspace it allocated for
-// this purpose.  This entry point allocates nothing: the sampler's scratch
-// (work-queue head, error word, per-item log terms, rows of hot words) lives
-// in `g_sample_scratch`, a file-scope device array that every GPU which loads
-// the library holds until the process exits.
+// Who needs it: a serving process whose own pool allocator reserved all
+// device memory up front and lets no library call cudaMalloc cannot hand
+// culda_sample a workspace allocated for this purpose.  This entry point
+// allocates nothing: the sampler's scratch (work-queue head, error word,
+// per-item log terms, rows of hot words) lives in `g_sample_scratch`, a
+// file-scope device array that every GPU which loads the library holds until
+// the process exits.  Each call still reads culda_sample's theta range check
+// back to the host, so it returns only once its stream has drained.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -31,7 +31,8 @@ void *g_scratch_addr[kMaxDevices] = {};
 
 // Device address of the scratch on the current device, looked up once per
 // device (the lookup loads the library's device code on that device if it is
-// not loaded yet).
+// not loaded yet) and kept for the life of the process: a cudaDeviceReset
+// unloads the module, after which the kept address is stale.
 int scratch_address(void **out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -62,6 +63,12 @@ int scratch_address(void **out) {
 extern "C" int culda_sample_noalloc(const culda_sample_args *a, void *stream) {
     if (!a) {
         culda::set_global_error("culda_sample_noalloc: null arguments");
+        return CULDA_ERR_INVALID_ARG;
+    }
+    // reject malformed sizes before they reach the size arithmetic below
+    if (a->k < 32 || a->k > 4096 || (a->k % 32) != 0 || a->num_items <= 0 || a->num_hot < 0) {
+        culda::set_global_error("culda_sample_noalloc: invalid argument (k %d, num_items %d, num_hot %d)", a->k,
+                                a->num_items, a->num_hot);
         return CULDA_ERR_INVALID_ARG;
     }
     const size_t need = culda_sample_workspace(a->k, a->num_items, a->num_hot);

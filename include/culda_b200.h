@@ -394,19 +394,23 @@ int culda_sample(const culda_sample_args *a, void *d_workspace, size_t workspace
 #define CULDA_NOALLOC_SCRATCH_BYTES (8u << 20)
 
 /* culda_sample without a caller workspace; no counterpart in the reference.
- * For callers that cannot allocate device memory for the sampler: an
- * application whose own pool allocator owns all device memory and does not
- * let libraries call cudaMalloc, or a latency-sensitive loop that cannot pay
- * the device-wide synchronisation of an allocation.  Same arguments, checks
- * and results as culda_sample; the scratch is a fixed device array of
+ * For callers that cannot allocate device memory for the sampler: a serving
+ * process whose own pool allocator reserved all device memory up front and
+ * lets no library call cudaMalloc.  Same arguments, checks and results as
+ * culda_sample; the scratch is a fixed device array of
  * CULDA_NOALLOC_SCRATCH_BYTES instead of a workspace, and the call allocates
- * nothing.  A work list needing more scratch than that (culda_sample_workspace)
- * is rejected with CULDA_ERR_UNSUPPORTED.  The first call on each device looks
- * up the array's device address (and loads the library's device code there if
- * that has not happened yet): make that first call before any stream capture.
- * Every call on a device shares the one array, so calls that may overlap on
- * the GPU (other streams, other host threads) race and must be serialised by
- * the caller. */
+ * nothing.  Invalid arguments (K, num_items <= 0, num_hot < 0) return
+ * CULDA_ERR_INVALID_ARG; a valid work list needing more scratch than the
+ * array holds (culda_sample_workspace) is rejected with CULDA_ERR_UNSUPPORTED.
+ * Like culda_sample, each call reads the theta range check back to the host,
+ * so it returns only after its stream has run the work queued before it.
+ * The first call on each device looks up the array's device address (and
+ * loads the library's device code there if that has not happened yet): make
+ * that first call before any stream capture.  The address is kept for the
+ * life of the process, so the library must not be used on a device after a
+ * cudaDeviceReset of it.  Every call on a device shares the one array, so
+ * calls that may overlap on the GPU (other streams, other host threads) race
+ * and must be serialised by the caller. */
 int culda_sample_noalloc(const culda_sample_args *a, void *stream);
 
 /* Replaces LDATrainPerplexity (src_culda/kernel/lda_train_kernel.cu:323-356):

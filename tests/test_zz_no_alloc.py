@@ -1,7 +1,7 @@
 """culda_sample_noalloc: the kernel-level sampler with its scratch in a fixed
 device array, for callers that cannot allocate device memory for a workspace
-(an application whose own pool allocator owns all device memory, or a loop
-that cannot pay an allocation's device-wide synchronisation).
+(a serving process whose own pool allocator reserved all device memory up
+front and lets no library call cudaMalloc).
 
 Two calls in a row must give the same topics and log-likelihood as
 culda_sample with a workspace on the same inputs: the array keeps the last
@@ -41,7 +41,8 @@ def _run(fn, p, a):
     return host(p.d["z_out"], np.uint16).copy(), ll.value
 
 
-def test_noalloc_matches_workspace_sampler_twice():
+@pytest.mark.parametrize("group_lanes", [_ffi.CULDA_SAMPLER_FLAT, 8], ids=["flat", "g8"])
+def test_noalloc_matches_workspace_sampler_twice(group_lanes):
     import torch
 
     if not torch.cuda.is_available():
@@ -52,7 +53,7 @@ def test_noalloc_matches_workspace_sampler_twice():
     p = prepare(c, k, MINI.alpha, MINI.beta, O.init_topics(c.num_tokens, k, 8), item_tokens=200)
     assert p.num_hot > 0  # the hot-row part of the scratch is exercised too
     assert update_theta(p) == 0
-    a = sample_args(p, seed=77, iteration=5, group_lanes=8)
+    a = sample_args(p, seed=77, iteration=5, group_lanes=group_lanes)
     need = lib.culda_sample_workspace(k, p.num_items, p.num_hot)
     assert need <= _ffi.CULDA_NOALLOC_SCRATCH_BYTES
     ws = torch.zeros(need // 4 + 64, dtype=torch.int32, device="cuda")
@@ -74,3 +75,16 @@ def test_noalloc_rejects_work_lists_beyond_the_array():
     assert lib.culda_sample_workspace(1024, 2_000_000, 0) > _ffi.CULDA_NOALLOC_SCRATCH_BYTES
     assert lib.culda_sample_noalloc(C.byref(a), None) == _ffi.CULDA_ERR_UNSUPPORTED
     assert b"fixed device array" in lib.culda_last_error(None)
+
+
+def test_noalloc_rejects_malformed_sizes():
+    """Negative sizes are argument errors, not oversize work lists."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    lib = cb.lib()
+    for kw in ({"k": 1024, "num_items": -1, "num_hot": 0}, {"k": 1024, "num_items": 10, "num_hot": -5},
+               {"k": -32, "num_items": 10, "num_hot": 0}):
+        a = _ffi.SampleArgs(**kw)
+        assert lib.culda_sample_noalloc(C.byref(a), None) == _ffi.CULDA_ERR_INVALID_ARG, kw

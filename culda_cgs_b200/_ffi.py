@@ -47,7 +47,7 @@ class GenParams(C.Structure):
 
 class Params(C.Structure):
     _fields_ = [("k", i32), ("alpha", f32), ("beta", f32), ("seed", u64), ("device", i32), ("group_lanes", i32),
-                ("item_tokens", i32), ("flags", i32), ("sample_blocks", i32)]
+                ("item_tokens", i32), ("flags", i32), ("sample_blocks", i32), ("theta_min_len", i32)]
 
 
 class IterStats(C.Structure):
@@ -61,7 +61,7 @@ class Info(C.Structure):
                 ("group_lanes", i32), ("sample_grid", i32), ("sample_blocks", i32), ("theta_grid", i32),
                 ("kernels_per_iteration", i32),
                 ("theta_capacity", i64), ("device_bytes", i64), ("doc_term", f64), ("tuned", i32),
-                ("tune_ms", f32)]
+                ("tune_ms", f32), ("theta_min_len", i32), ("theta_long_docs", i32), ("theta_tune_ms", f32)]
 
 
 class Item(C.Structure):

@@ -38,13 +38,16 @@ using namespace culda;
 namespace {
 
 // ------------------------------------------------------------ autotuner
-// Sampler variants are timed on the context's initial state; the fastest is
-// kept.  Results are remembered per (device name, N, D, V, K): in the process,
-// and in the file named by CULDA_TUNE_CACHE (lines "key group_lanes
-// sample_blocks ms") when that variable is set.
+// Sampler variants and theta-rebuild bin thresholds are timed on the
+// context's state; the fastest of each is kept.  Results are remembered per
+// (device name, N, D, V, K): in the process, and in the file named by
+// CULDA_TUNE_CACHE (lines "key group_lanes sample_blocks ms theta_min_len")
+// when that variable is set.  theta_min_len 0 means every doc is rebuilt by
+// one warp.
 struct TuneResult {
     int group_lanes = 0, sample_blocks = 0;
     float ms = 0.f;
+    int theta_min_len = -1;  // -1: not tuned (a cache line written before the rebuild was tuned)
 };
 
 std::mutex g_tune_mu;
@@ -76,7 +79,9 @@ bool tune_lookup(const std::string &key, TuneResult &r) {
         std::istringstream ls(line);
         std::string k;
         TuneResult t;
-        if (ls >> k >> t.group_lanes >> t.sample_blocks >> t.ms && k == key && sample_variant_exists(t.group_lanes, t.sample_blocks)) {
+        if (ls >> k >> t.group_lanes >> t.sample_blocks >> t.ms && k == key &&
+            sample_variant_exists(t.group_lanes, t.sample_blocks)) {
+            if (!(ls >> t.theta_min_len) || t.theta_min_len < 0) t.theta_min_len = -1;
             r = t;
             found = true;  // the last line for a key wins
         }
@@ -91,7 +96,7 @@ void tune_store(const std::string &key, const TuneResult &r) {
     const char *path = std::getenv("CULDA_TUNE_CACHE");
     if (!path || !*path) return;
     std::ofstream f(path, std::ios::app);
-    f << key << ' ' << r.group_lanes << ' ' << r.sample_blocks << ' ' << r.ms << '\n';
+    f << key << ' ' << r.group_lanes << ' ' << r.sample_blocks << ' ' << r.ms << ' ' << r.theta_min_len << '\n';
 }
 
 }  // namespace
@@ -107,6 +112,31 @@ int fail(culda_ctx *c, int code, const char *fmt, ...) {
     return code;
 }
 
+
+// Queue counter of the theta rebuild's block bin: its own 64-byte line of the
+// counter array (slot 0 is the sampler's work queue).
+static int32_t *theta_queue(culda_ctx *ctx) { return ctx->d_counter + 16; }
+
+// Docs of at least min_len tokens (a prefix of the longest-first doc order).
+static int count_long_docs(const culda_ctx *ctx, int min_len) {
+    if (min_len <= 0) return 0;
+    int n = 0;
+    for (int d = 0; d < ctx->D; ++d) n += (ctx->h_doc_ptr[(size_t)d + 1] - ctx->h_doc_ptr[(size_t)d]) >= min_len;
+    return n;
+}
+
+static void set_theta_bins(culda_ctx *ctx, int min_len) {
+    ctx->theta_min_len = min_len > 0 ? min_len : 0;
+    ctx->theta_long = count_long_docs(ctx, ctx->theta_min_len);
+}
+
+// Default bin threshold: a doc whose tokens outnumber a warp's average share
+// of the corpus (N over the launch's warps) would hold its warp past the rest
+// of the launch, so it gets a whole CTA; never below 1024 tokens.
+static int default_theta_min_len(const culda_ctx *ctx) {
+    const int64_t warps = (int64_t)ctx->theta_grid * kThetaWarps;
+    return (int)std::min<int64_t>(65536, std::max<int64_t>(1024, ctx->N / std::max<int64_t>(1, warps)));
+}
 
 // Sampler parameters for topics d_z[cur] -> d_z[1-cur]; the Philox iteration
 // comes from the device counter when iteration_ptr is set (graph launches).
@@ -183,7 +213,7 @@ int record_iteration(culda_ctx *ctx, cudaStream_t s, int cur) {
     CK(record_event(ctx->ev_t0, s));
     CK(launch_theta_rebuild(ctx->K, ctx->D, ctx->d_doc_ptr, ctx->d_doc_tok, ctx->d_z[nxt], ctx->d_doc_order,
                             ctx->d_rows, ctx->d_theta, ctx->d_nk, &ctx->d_stats->row_entries, ctx->d_error,
-                            ctx->theta_grid, s));
+                            ctx->theta_grid, s, ctx->theta_long, theta_queue(ctx)));
     CK(record_event(ctx->ev_t1, s));
     copy_error_kernel<<<1, 1, 0, s>>>(ctx->d_error, ctx->d_stats);
     CK(cudaGetLastError());
@@ -200,7 +230,7 @@ int rebuild_counts(culda_ctx *ctx) {
     CK(cudaMemsetAsync(&ctx->d_stats->row_entries, 0, 3 * sizeof(int64_t), s));
     CK(launch_theta_rebuild(ctx->K, ctx->D, ctx->d_doc_ptr, ctx->d_doc_tok, ctx->d_z[ctx->cur], ctx->d_doc_order,
                             ctx->d_rows, ctx->d_theta, ctx->d_nk, &ctx->d_stats->row_entries, ctx->d_error,
-                            ctx->theta_grid, s));
+                            ctx->theta_grid, s, ctx->theta_long, theta_queue(ctx)));
     CK(cudaStreamSynchronize(s));
     int32_t e = 0;
     CK(cudaMemcpy(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost));
@@ -211,6 +241,50 @@ int rebuild_counts(culda_ctx *ctx) {
 namespace {
 
 constexpr uint32_t kTuneIteration = 3;
+
+// Times the theta rebuild of the current topics at each candidate bin
+// threshold (0 = warp per doc for every doc) and keeps the fastest.  The
+// rebuild of the same topics writes the same rows and n_k, so the state does
+// not change.
+int autotune_rebuild(culda_ctx *ctx, TuneResult &best) {
+    cudaStream_t s = ctx->stream;
+    const int dflt = default_theta_min_len(ctx);
+    const int cands[] = {0, dflt, 65535, 16384, 8192, 4096, 2048, 1024, 512, 256};
+    std::vector<int> seen_long;
+    float best_ms = 0.f;
+    int best_len = 0;
+    for (int len : cands) {
+        const int nl = count_long_docs(ctx, len);
+        if (len > 0 && nl == 0) continue;
+        if (std::find(seen_long.begin(), seen_long.end(), nl) != seen_long.end()) continue;  // same bins
+        seen_long.push_back(nl);
+        float t = 0.f;
+        for (int rep = 0; rep < 3; ++rep) {
+            CK(cudaMemsetAsync(ctx->d_nk, 0, sizeof(int32_t) * (size_t)ctx->K, s));
+            CK(cudaMemsetAsync(&ctx->d_stats->row_entries, 0, 3 * sizeof(int64_t), s));
+            CK(cudaEventRecord(ctx->ev0, s));
+            CK(launch_theta_rebuild(ctx->K, ctx->D, ctx->d_doc_ptr, ctx->d_doc_tok, ctx->d_z[ctx->cur],
+                                    ctx->d_doc_order, ctx->d_rows, ctx->d_theta, ctx->d_nk,
+                                    &ctx->d_stats->row_entries, ctx->d_error, ctx->theta_grid, s, nl,
+                                    theta_queue(ctx)));
+            CK(cudaEventRecord(ctx->ev1, s));
+            CK(cudaEventSynchronize(ctx->ev1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            if (rep == 1 || (rep == 2 && ms < t)) t = ms;
+        }
+        if (ctx->params.flags & CULDA_FLAG_VERBOSE)
+            fprintf(stderr, "culda: autotune theta_min_len=%d (%d docs by a CTA): %.3f ms\n", len, nl, t);
+        if (best_ms == 0.f || t < best_ms) {
+            best_ms = t;
+            best_len = len;
+        }
+    }
+    best.theta_min_len = best_len;
+    set_theta_bins(ctx, best_len);
+    ctx->theta_tune_ms = best_ms;
+    return CULDA_OK;
+}
 
 // Times each sampler variant on the current state: hot rows and
 // uniforms once, then per variant one warm-up and two timed launches that
@@ -231,6 +305,7 @@ int autotune_sampler(culda_ctx *ctx) {
             ctx->sample_grid = std::max(1, std::min(ctx->num_items, num_sms(ctx->device) * bps));
             ctx->tuned = 2;
             ctx->tune_ms = best.ms;
+            if (best.theta_min_len >= 0) set_theta_bins(ctx, best.theta_min_len);
             return CULDA_OK;
         }
     }
@@ -278,6 +353,10 @@ int autotune_sampler(culda_ctx *ctx) {
                                                                                  best.sample_blocks)));
     ctx->tuned = 1;
     ctx->tune_ms = best.ms;
+    const int rc = autotune_rebuild(ctx, best);
+    if (rc) return rc;
+    CK(cudaMemcpy(&e, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (e) return fail(ctx, CULDA_ERR_DEVICE_STATE, "autotune: theta rebuild reported device error 0x%x", e);
     tune_store(key, best);
     return CULDA_OK;
 }
@@ -564,8 +643,9 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: alpha and beta must be positive");
     if (p->item_tokens < 0 || p->item_tokens > 65535)
         return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: item_tokens=%d outside 0..65535", p->item_tokens);
-    if ((p->flags & CULDA_FLAG_AUTOTUNE) && (p->group_lanes != 0 || p->sample_blocks != 0))
-        return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: CULDA_FLAG_AUTOTUNE needs group_lanes = sample_blocks = 0");
+    if ((p->flags & CULDA_FLAG_AUTOTUNE) && (p->group_lanes != 0 || p->sample_blocks != 0 || p->theta_min_len != 0))
+        return fail(ctx, CULDA_ERR_INVALID_ARG,
+                    "culda_create: CULDA_FLAG_AUTOTUNE needs group_lanes = sample_blocks = theta_min_len = 0");
     const int gl = pick_group_lanes(p->group_lanes, p->k);
     if (gl == 0) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_create: group_lanes=%d", p->group_lanes);
     const int sb = pick_sample_blocks(p->sample_blocks, gl);
@@ -689,6 +769,8 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     int tbps = theta_blocks_per_sm(K);
     if (tbps <= 0) tbps = 1;
     ctx->theta_grid = std::max(1, std::min(sms * tbps, (D + kThetaWarps - 1) / kThetaWarps));
+    set_theta_bins(ctx, p->theta_min_len > 0 ? p->theta_min_len
+                        : p->theta_min_len < 0 ? 0 : default_theta_min_len(ctx));
     // work items: words, hot words split so no item exceeds a quarter of a CTA's share
     std::vector<culda_item> items, hot;
     {
@@ -1173,6 +1255,9 @@ extern "C" int culda_get_info(const culda_ctx *ctx, culda_info *info) {
     info->sample_blocks = ctx->sample_blocks;
     info->tuned = ctx->tuned;
     info->tune_ms = ctx->tune_ms;
+    info->theta_min_len = ctx->theta_min_len;
+    info->theta_long_docs = ctx->theta_long;
+    info->theta_tune_ms = ctx->theta_tune_ms;
     info->theta_grid = ctx->theta_grid;
     // hot_rows (when words are split), uniforms, sample, finalize_ll, theta_rebuild, copy_error
     info->kernels_per_iteration = (ctx->num_hot > 0 ? 1 : 0) + 5;

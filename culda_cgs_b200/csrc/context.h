@@ -52,6 +52,10 @@ struct culda_ctx {
     size_t block_bytes = 0;
 
     int sample_grid = 1, theta_grid = 1;
+    // theta rebuild bins: docs of at least theta_min_len tokens (the first
+    // theta_long of d_doc_order) are rebuilt a CTA each, the rest a warp each
+    int theta_min_len = 0, theta_long = 0;
+    float theta_tune_ms = 0.f;  // the chosen threshold's rebuild time when it was timed
     double doc_term = 0;  // sum_d L_d * log(L_d + K alpha)
     std::vector<int64_t> h_doc_ptr;
     std::vector<int32_t> h_max_ia;

@@ -9,9 +9,10 @@
 //   hot_rows_kernel      full phi rows of words split over several work items
 //   sample_kernel<G>     the draw (sampler.cu)
 //   finalize_ll_kernel   fixed-order sum of the per-item log terms
-//   theta_rebuild_kernel warp per doc (longest first): 16-bit shared-memory
-//                        histogram of the doc's new topics, CSR compaction in
-//                        ascending topic, zero padding, n_k as a column sum.
+//   theta_rebuild_kernel block per long doc, warp per other doc (longest
+//                        first): 16-bit shared-memory histogram of the doc's
+//                        new topics, CSR compaction in ascending topic, zero
+//                        padding, n_k as a column sum.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,17 +26,111 @@
 namespace culda {
 
 // ---------------------------------------------------------- theta rebuild
-// Warp per doc.  Shared memory per warp: K/2 words of packed 16-bit counts
-// (a topic can hold at most L_d <= 65535 tokens, so a low half never carries
-// into the high half) and K/32 words of a non-zero mask; per block: K n_k
-// partial counts.  The compaction walks the mask in ascending topic order, so
-// each row comes out sorted as lda_theta_kernel.cu:58-85 leaves it, and only
-// the touched count words are cleared again.
+// Two bins in one persistent launch.  The longest documents (the first
+// num_long of doc_order, every one at least the bin threshold long) are taken
+// one at a time by a whole CTA from an atomic queue: its eight warps count
+// the doc's tokens into one shared histogram.  Every other document is taken
+// by one warp (static round robin over the rest of doc_order, longest first).
+// Shared memory per warp: K/2 words of packed 16-bit counts (a topic can hold
+// at most L_d <= 65535 tokens, so a low half never carries into the high half)
+// and K/32 words of a non-zero mask; per block: K n_k partial counts.  The
+// block bin uses warp 0's histogram.  The compaction walks the mask in
+// ascending topic order, so each row comes out sorted as
+// lda_theta_kernel.cu:58-85 leaves it, and only the touched count words are
+// cleared again.
+
+namespace {
+
+// Counts tokens [b + first, e) with stride `step` into the packed histogram.
+__device__ __forceinline__ void theta_count(int K, int64_t b, int64_t e, int first, int step,
+                                            const int32_t *__restrict__ doc_tok,
+                                            const uint16_t *__restrict__ topics, uint32_t *cnt, uint32_t *mask,
+                                            int32_t *error) {
+    // eight tokens per thread in flight: the index loads, then the topic
+    // loads they address, then the histogram updates
+    constexpr int kInFlight = 8;
+    for (int64_t j0 = b + first; j0 < e; j0 += (int64_t)step * kInFlight) {
+        int32_t idx[kInFlight];
+        uint32_t zz[kInFlight];
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) idx[u] = j0 + (int64_t)step * u < e ? doc_tok[j0 + (int64_t)step * u] : -1;
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) zz[u] = idx[u] >= 0 ? (uint32_t)topics[idx[u]] : 0u;
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            if (idx[u] < 0) continue;
+            const uint32_t z = zz[u];
+            if (z >= (uint32_t)K) {
+                atomicOr(error, kErrTopicRange);
+                continue;
+            }
+            const uint32_t sh = (z & 1u) << 4;
+            const uint32_t old = atomicAdd(&cnt[z >> 1], 1u << sh);
+            if (((old >> sh) & 0xFFFFu) == 0u) atomicOr(&mask[z >> 5], 1u << (z & 31u));
+        }
+    }
+}
+
+// One warp: the doc's row from its histogram (ascending topic), zero padding
+// to the row's previous end, the histogram cleared, n_k partial sums.
+__device__ __forceinline__ void theta_compact(int K, int d, int64_t len, int lane, uint32_t *cnt, uint32_t *mask,
+                                              uint32_t *nk_acc, int2 *rows, ThetaEntry *theta, int64_t &my_rows,
+                                              int64_t &my_nnz, int64_t &my_tok_nnz) {
+    const int mwords = K >> 5;
+    const int2 row = rows[d];
+    const int start = row.x, old_end = row.y;
+    int nnz = 0;
+    for (int mb = 0; mb < mwords; mb += 32) {
+        const int mi = mb + lane;
+        const uint32_t mw = mi < mwords ? mask[mi] : 0u;
+        const int pc = __popc(mw);
+        int incl = pc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        int pos = start + nnz + incl - pc;
+        uint32_t bits = mw;
+        while (bits) {
+            const int bit = __ffs(bits) - 1;
+            bits &= bits - 1u;
+            const uint32_t z = ((uint32_t)mi << 5) | (uint32_t)bit;
+            const uint32_t c = (cnt[z >> 1] >> ((z & 1u) << 4)) & 0xFFFFu;
+            theta[pos++] = theta_entry(z, c);
+            atomicAdd(&nk_acc[z], c);
+        }
+        __syncwarp();
+        bits = mw;
+        while (bits) {
+            const int bit = __ffs(bits) - 1;
+            bits &= bits - 1u;
+            cnt[(((uint32_t)mi << 5) | (uint32_t)bit) >> 1] = 0u;
+        }
+        if (mi < mwords) mask[mi] = 0u;
+        nnz += total;
+    }
+    __syncwarp();
+    const int new_end = start + ((nnz + 31) & ~31);
+    const int zend = max(new_end, old_end);
+    for (int j = start + nnz + lane; j < zend; j += 32) theta[j] = 0u;
+    if (lane == 0) {
+        rows[d].y = new_end;
+        my_rows += len * (int64_t)(new_end - start);
+        my_nnz += nnz;
+        my_tok_nnz += len * (int64_t)nnz;
+    }
+}
+
+}  // namespace
+
 __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
     int K, int num_docs, const int64_t *__restrict__ doc_ptr, const int32_t *__restrict__ doc_tok,
-    const uint16_t *__restrict__ topics, const int32_t *__restrict__ doc_order, int2 *rows, ThetaEntry *theta,
-    int32_t *nk, int64_t *stats, int32_t *error) {
+    const uint16_t *__restrict__ topics, const int32_t *__restrict__ doc_order, int num_long, int32_t *long_queue,
+    int2 *rows, ThetaEntry *theta, int32_t *nk, int64_t *stats, int32_t *error) {
     extern __shared__ uint32_t sm_u32[];
+    __shared__ int s_next;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cwords = K >> 1, mwords = K >> 5;
     uint32_t *nk_acc = sm_u32;
@@ -46,82 +141,41 @@ __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
     __syncthreads();
 
     int64_t my_rows = 0, my_nnz = 0, my_tok_nnz = 0;
+    // block bin: one long document per CTA at a time
+    if (num_long > 0) {
+        uint32_t *bcnt = sm_u32 + K;  // warp 0's histogram
+        uint32_t *bmask = bcnt + cwords;
+        for (;;) {
+            if (threadIdx.x == 0) s_next = atomicAdd(long_queue, 1);
+            __syncthreads();
+            const int i = s_next;
+            __syncthreads();  // every thread has read s_next before thread 0 overwrites it
+            if (i >= num_long) break;
+            const int d = doc_order[i];
+            const int64_t b = doc_ptr[d], e = doc_ptr[d + 1];
+            if (e - b > 65535) {
+                if (threadIdx.x == 0) atomicOr(error, kErrLongDoc);
+                continue;
+            }
+            theta_count(K, b, e, threadIdx.x, kThetaWarps * 32, doc_tok, topics, bcnt, bmask, error);
+            __syncthreads();
+            if (warp == 0) theta_compact(K, d, e - b, lane, bcnt, bmask, nk_acc, rows, theta, my_rows, my_nnz,
+                                         my_tok_nnz);
+            __syncthreads();  // the histogram is clear again before the next document
+        }
+    }
+    // warp bin: the remaining documents, one per warp
     const int nw = gridDim.x * kThetaWarps;
-    for (int i = blockIdx.x * kThetaWarps + warp; i < num_docs; i += nw) {
+    for (int i = num_long + blockIdx.x * kThetaWarps + warp; i < num_docs; i += nw) {
         const int d = doc_order ? doc_order[i] : i;
         const int64_t b = doc_ptr[d], e = doc_ptr[d + 1];
         if (e - b > 65535) {
             if (lane == 0) atomicOr(error, kErrLongDoc);
             continue;
         }
-        // eight tokens per lane in flight: the index loads, then the topic
-        // loads they address, then the histogram updates
-        constexpr int kInFlight = 8;
-        for (int64_t j0 = b + lane; j0 < e; j0 += 32 * kInFlight) {
-            int32_t idx[kInFlight];
-            uint32_t zz[kInFlight];
-#pragma unroll
-            for (int u = 0; u < kInFlight; ++u) idx[u] = j0 + 32 * u < e ? doc_tok[j0 + 32 * u] : -1;
-#pragma unroll
-            for (int u = 0; u < kInFlight; ++u) zz[u] = idx[u] >= 0 ? (uint32_t)topics[idx[u]] : 0u;
-#pragma unroll
-            for (int u = 0; u < kInFlight; ++u) {
-                if (idx[u] < 0) continue;
-                const uint32_t z = zz[u];
-                if (z >= (uint32_t)K) {
-                    atomicOr(error, kErrTopicRange);
-                    continue;
-                }
-                const uint32_t sh = (z & 1u) << 4;
-                const uint32_t old = atomicAdd(&cnt[z >> 1], 1u << sh);
-                if (((old >> sh) & 0xFFFFu) == 0u) atomicOr(&mask[z >> 5], 1u << (z & 31u));
-            }
-        }
+        theta_count(K, b, e, lane, 32, doc_tok, topics, cnt, mask, error);
         __syncwarp();
-        const int2 row = rows[d];
-        const int start = row.x, old_end = row.y;
-        int nnz = 0;
-        for (int mb = 0; mb < mwords; mb += 32) {
-            const int mi = mb + lane;
-            const uint32_t mw = mi < mwords ? mask[mi] : 0u;
-            const int pc = __popc(mw);
-            int incl = pc;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            int pos = start + nnz + incl - pc;
-            uint32_t bits = mw;
-            while (bits) {
-                const int bit = __ffs(bits) - 1;
-                bits &= bits - 1u;
-                const uint32_t z = ((uint32_t)mi << 5) | (uint32_t)bit;
-                const uint32_t c = (cnt[z >> 1] >> ((z & 1u) << 4)) & 0xFFFFu;
-                theta[pos++] = theta_entry(z, c);
-                atomicAdd(&nk_acc[z], c);
-            }
-            __syncwarp();
-            bits = mw;
-            while (bits) {
-                const int bit = __ffs(bits) - 1;
-                bits &= bits - 1u;
-                cnt[(((uint32_t)mi << 5) | (uint32_t)bit) >> 1] = 0u;
-            }
-            if (mi < mwords) mask[mi] = 0u;
-            nnz += total;
-        }
-        __syncwarp();
-        const int new_end = start + ((nnz + 31) & ~31);
-        const int zend = max(new_end, old_end);
-        for (int j = start + nnz + lane; j < zend; j += 32) theta[j] = 0u;
-        if (lane == 0) {
-            rows[d].y = new_end;
-            my_rows += (e - b) * (int64_t)(new_end - start);
-            my_nnz += nnz;
-            my_tok_nnz += (e - b) * (int64_t)nnz;
-        }
+        theta_compact(K, d, e - b, lane, cnt, mask, nk_acc, rows, theta, my_rows, my_nnz, my_tok_nnz);
     }
     __syncthreads();
     if (nk)
@@ -150,12 +204,19 @@ int theta_blocks_per_sm(int k) {
 
 cudaError_t launch_theta_rebuild(int k, int num_docs, const int64_t *doc_ptr, const int32_t *doc_tok,
                                  const uint16_t *topics, const int32_t *doc_order, int2 *rows, ThetaEntry *theta,
-                                 int32_t *nk, int64_t *stats, int32_t *error, int grid, cudaStream_t s) {
+                                 int32_t *nk, int64_t *stats, int32_t *error, int grid, cudaStream_t s,
+                                 int num_long, int32_t *long_queue) {
+    if (num_long > 0 && (!doc_order || !long_queue || num_long > num_docs)) return cudaErrorInvalidValue;
     const size_t smem = theta_smem_bytes(k);
     cudaError_t e = allow_smem(reinterpret_cast<const void *>(&theta_rebuild_kernel), smem, s);
     if (e != cudaSuccess) return e;
-    theta_rebuild_kernel<<<grid, kThetaWarps * 32, smem, s>>>(k, num_docs, doc_ptr, doc_tok, topics, doc_order, rows,
-                                                              theta, nk, stats, error);
+    if (num_long > 0) {
+        e = cudaMemsetAsync(long_queue, 0, sizeof(int32_t), s);
+        if (e != cudaSuccess) return e;
+    }
+    theta_rebuild_kernel<<<grid, kThetaWarps * 32, smem, s>>>(k, num_docs, doc_ptr, doc_tok, topics, doc_order,
+                                                              num_long > 0 ? num_long : 0, long_queue, rows, theta,
+                                                              nk, stats, error);
     return cudaGetLastError();
 }
 

@@ -79,9 +79,13 @@ cudaError_t launch_sample(const SampleParams &p, int group_lanes, int blocks_per
 
 size_t theta_smem_bytes(int k);
 int theta_blocks_per_sm(int k);
+// The first num_long docs of doc_order (which must then be given) are taken
+// a whole CTA each from the queue counter long_queue (cleared by the launch);
+// the rest one warp each.
 cudaError_t launch_theta_rebuild(int k, int num_docs, const int64_t *doc_ptr, const int32_t *doc_tok,
                                  const uint16_t *topics, const int32_t *doc_order, int2 *rows, ThetaEntry *theta,
-                                 int32_t *nk, int64_t *stats, int32_t *error, int grid, cudaStream_t s);
+                                 int32_t *nk, int64_t *stats, int32_t *error, int grid, cudaStream_t s,
+                                 int num_long = 0, int32_t *long_queue = nullptr);
 
 cudaError_t launch_hot_rows(int k, const culda_item *hot_items, int num_hot_items, const uint16_t *topics,
                             int32_t *hot_phi, int32_t *error, cudaStream_t s);

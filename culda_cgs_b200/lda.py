@@ -44,7 +44,8 @@ class LDA:
     """One corpus resident on one GPU (culda_create ... culda_destroy)."""
 
     def __init__(self, corpus: Corpus, k: int, alpha: float, beta: float, seed: int = 1, device: int = 0,
-                 group_lanes: int = 0, item_tokens: int = 0, flags: int = 0, sample_blocks: int = 0):
+                 group_lanes: int = 0, item_tokens: int = 0, flags: int = 0, sample_blocks: int = 0,
+                 theta_min_len: int = 0):
         self.corpus = corpus
         self.k = int(k)
         self.alpha = float(np.float32(alpha))
@@ -53,7 +54,8 @@ class LDA:
         self.num_docs = corpus.num_docs
         self.num_words = corpus.num_words
         self.seed = int(seed)
-        p = _ffi.Params(self.k, alpha, beta, seed, device, group_lanes, item_tokens, flags, sample_blocks)
+        p = _ffi.Params(self.k, alpha, beta, seed, device, group_lanes, item_tokens, flags, sample_blocks,
+                        theta_min_len)
         self._ctx = C.c_void_p()
         check(lib().culda_create(corpus.c_ptr, C.byref(p), C.byref(self._ctx)))
 

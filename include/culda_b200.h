@@ -183,6 +183,12 @@ typedef struct culda_params {
                               for the flat walk, 8 for the group samplers), 8 (<= 64
                               registers), or 10 (<= 48 registers; the flat walk and
                               group_lanes 4, 8, 16) */
+    int32_t theta_min_len; /* theta rebuild bins: docs of at least this many tokens are rebuilt
+                              by a whole CTA each, the others by one warp each.  0 = auto (N
+                              over the rebuild's warps, at least 1024; CULDA_FLAG_AUTOTUNE
+                              times candidates), -1 = one warp for every doc, > 0 = this
+                              threshold.  No reference counterpart (the reference's rebuild
+                              takes a warp per doc, lda_theta_kernel.cu:5-87). */
 } culda_params;
 
 /* group_lanes value of the warp-flattened sampler: a warp splits the rows of up
@@ -194,12 +200,13 @@ enum {
     CULDA_FLAG_NO_GRAPH = 1,      /* launch the iteration kernel by kernel instead of one CUDA graph */
     CULDA_FLAG_VERBOSE = 2,       /* print set-up details to stderr */
     CULDA_FLAG_NO_REORDER = 4,    /* keep tokens in input order inside each word (default: by doc length) */
-    CULDA_FLAG_AUTOTUNE = 8       /* time the sampler variants (lanes per token x register budget) on the
-                                     state before iteration 3 (after two iterations with the default
-                                     variant) and keep the fastest; group_lanes and sample_blocks must be
-                                     0.  Results are cached per (device name, N, D, V, K) in the process
-                                     and, when the environment variable CULDA_TUNE_CACHE names a file, in
-                                     that file; a cached result applies from the first iteration. */
+    CULDA_FLAG_AUTOTUNE = 8       /* time the sampler variants (lanes per token x register budget) and
+                                     the theta rebuild's bin thresholds on the state before iteration 3
+                                     (after two iterations with the defaults) and keep the fastest;
+                                     group_lanes, sample_blocks and theta_min_len must be 0.  Results
+                                     are cached per (device name, N, D, V, K) in the process and, when
+                                     the environment variable CULDA_TUNE_CACHE names a file, in that
+                                     file; a cached result applies from the first iteration. */
 };
 
 typedef struct culda_iter_stats {
@@ -283,6 +290,9 @@ typedef struct culda_info {
     int32_t tuned;              /* sampler variant: 0 = given or default (or tuning still pending),
                                    1 = timed, 2 = from the tuning cache */
     float tune_ms;              /* the chosen variant's sampler time when it was timed (tuned != 0) */
+    int32_t theta_min_len;      /* theta rebuild bin threshold in tokens (0: every doc by one warp) */
+    int32_t theta_long_docs;    /* docs rebuilt by a whole CTA each */
+    float theta_tune_ms;        /* the chosen threshold's rebuild time when it was timed, else 0 */
 } culda_info;
 
 int culda_get_info(const culda_ctx *ctx, culda_info *info);

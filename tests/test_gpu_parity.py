@@ -233,3 +233,39 @@ def test_longest_allowed_document():
     with cb.LDA(c, 64, 0.1, 0.01, seed=2) as m:
         m.iterate(1)
         assert_counts_exact(m, c)
+
+
+@pytest.mark.parametrize("min_len", [1, 40, 300, -1])
+@pytest.mark.parametrize("k", [64, 1024])
+def test_theta_rebuild_bins_match_the_oracle(corpora, min_len, k):
+    """Docs of at least min_len tokens rebuilt by a whole CTA each (1: every
+    doc; -1: none): theta, n_k and the draws still match the oracle."""
+    c = corpora[id(MINI.gen)]
+    seed = 808
+    with cb.LDA(c, k, 50.0 / k, 0.01, seed=seed, theta_min_len=min_len) as m:
+        info = m.info()
+        L = np.diff(c.doc_ptr)
+        assert info["theta_min_len"] == max(min_len, 0)
+        assert info["theta_long_docs"] == (int((L >= min_len).sum()) if min_len > 0 else 0)
+        s0 = assert_counts_exact(m, c)
+        z1_ora, margin, ll0 = s0.sample(seed, 1)
+        st = m.iterate(1)[0]
+        assert st["status"] == 0
+        assert_ll_close(st["loglik"], ll0)
+        assert_draws_match(m.topics(), z1_ora, margin)
+        s1 = assert_counts_exact(m, c)
+        assert st["theta_nnz"] == int((s1.theta_a != 0).sum())
+        assert st["row_entries"] == int((L * (s1.cur_ia - s1.max_ia[:-1])).sum())
+        m.iterate(2)
+        assert_counts_exact(m, c)
+
+
+def test_theta_rebuild_block_bin_on_the_longest_document():
+    """The 65535-token document (the 16-bit count limit) rebuilt by a CTA."""
+    n = 65535
+    doc_ids = np.r_[np.zeros(n, dtype=np.int32), np.ones(3, dtype=np.int32)]
+    c = cb.Corpus.from_arrays(np.array([0, n, n + 3]), np.array([0, n // 2, n + 3]), doc_ids)
+    with cb.LDA(c, 64, 0.1, 0.01, seed=2, theta_min_len=1000) as m:
+        assert m.info()["theta_long_docs"] == 1
+        m.iterate(1)
+        assert_counts_exact(m, c)

@@ -482,6 +482,51 @@ def run_ours(args, world, rank, local, pg):
     return line
 
 
+# ------------------------------------------------- doc-chunk data parallel
+def run_dp(args, world, rank, local, pg):
+    """--mode dp: one corpus split into `world` token-balanced doc chunks, one
+    per rank (the reference's -g N -c N); every iteration each rank samples its
+    chunk against the summed counts, then the chunks' counts are summed by an
+    NCCL all-reduce.  Total work is fixed (strong scaling); the step time is
+    the slowest rank's, on CUDA events around sample + rebuild + exchange."""
+    import torch
+
+    import culda_cgs_b200 as cb
+    from culda_cgs_b200.chunked import ChunkedLDA
+
+    wl = workload(args, args.seed)
+    corpus = cb.Corpus.generate(wl.gen)
+    N = corpus.num_tokens
+    dp = ChunkedLDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed, rank=rank, world=world, device=local)
+    log(f"[rank {rank}] chunk docs {dp.doc_range} tokens {dp.chunk.num_tokens} of {N}")
+    dp.iterate(args.warmup)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    cuda_sync()
+    clocks.mark_start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    stats = dp.iterate(args.steps)
+    ev1.record()
+    cuda_sync()
+    barrier(pg)
+    clocks.mark_end()
+    clk = clocks.stop()
+    seconds = allreduce_max(pg, ev0.elapsed_time(ev1) / 1e3)
+    dp.close()
+    return {
+        "metric": METRIC, "value": N * args.steps / seconds, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * seconds / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded generator, shapes of the workload)",
+        "config": common_config(wl, N, corpus.num_docs, corpus.num_words, args.seed, world)
+        | {"parallelism": f"doc-chunk dp{world} (NCCL all-reduce of V*K+K int32 counts per iteration)"},
+        "clocks": clk, "loglik": [round(s["loglik_global"], 8) for s in stats],
+        "exchange_bytes_per_step": 4 * (corpus.num_words * wl.k + wl.k),
+    }
+
+
 # -------------------------------------------------------------- reference
 ITER_RE = re.compile(r"Iteration\s+(\d+):\s+([\d.]+) sec,\s+([\d.]+) sec, logLikelyhood = ([-\d.naninf]+),\s+([\d.]+) M")
 
@@ -569,6 +614,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["replicas", "dp"], default="replicas",
+                    help="N > 1: independent replicas (default) or doc-chunk data parallelism")
     ap.add_argument("--workload", default="plain-cgs-scale")
     ap.add_argument("--k", type=int, default=0, help="topics (default: the workload's); alpha = 50/K")
     ap.add_argument("--seed", type=int, default=1)
@@ -593,6 +640,8 @@ def main():
     try:
         if args.impl == "reference":
             line = run_reference(args, world, rank)
+        elif args.mode == "dp":
+            line = run_dp(args, world, rank, local, pg)
         else:
             line = run_ours(args, world, rank, local, pg)
         if rank == 0 and line is not None:

@@ -161,6 +161,8 @@ SIGNATURES = {
     "culda_next_iteration": (u32, [C.c_void_p]),
     "culda_set_iteration": (C.c_int, [C.c_void_p, u32]),
     "culda_warm_start": (C.c_int, [C.c_void_p]),
+    "culda_count_phi": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "culda_set_shared_phi": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -81,6 +81,8 @@ struct culda_ctx {
     // model), used by the samplers instead of the counts of this corpus.
     int32_t *d_frozen_phi = nullptr;  // [V x K]
     int32_t *d_frozen_nk = nullptr;   // [K]
+    // the two above are the caller's (culda_set_shared_phi), not freed here
+    bool frozen_borrowed = false;
 };
 
 // Records the message of a failed call on the context (and thread-locally) and

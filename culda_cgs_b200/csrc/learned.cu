@@ -488,9 +488,11 @@ int check_device_error(culda_ctx *ctx, const char *what) {
 
 void free_learned_state(culda_ctx *ctx) {
     void *bufs[] = {ctx->d_doc_words, ctx->d_acc,    ctx->d_ndk,        ctx->d_cdf,        ctx->d_cdf_blk,
-                    ctx->d_probs,     ctx->d_mh_stats, ctx->d_frozen_phi, ctx->d_frozen_nk};
+                    ctx->d_probs,     ctx->d_mh_stats, ctx->frozen_borrowed ? nullptr : ctx->d_frozen_phi,
+                    ctx->frozen_borrowed ? nullptr : ctx->d_frozen_nk};
     for (void *b : bufs)
         if (b) cudaFree(b);
+    ctx->frozen_borrowed = false;
     ctx->d_doc_words = nullptr;
     ctx->d_acc = nullptr;
     ctx->d_ndk = nullptr;
@@ -743,6 +745,11 @@ extern "C" int culda_set_frozen_phi(culda_ctx *ctx, const int32_t *phi, const in
     if (!ctx) return fail(ctx, CULDA_ERR_INVALID_ARG, "culda_set_frozen_phi: null context");
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->frozen_borrowed) {  // shared counts of a chunked run: the caller's buffers
+        ctx->d_frozen_phi = nullptr;
+        ctx->d_frozen_nk = nullptr;
+        ctx->frozen_borrowed = false;
+    }
     if (!phi) {
         if (ctx->d_frozen_phi) cudaFree(ctx->d_frozen_phi);
         if (ctx->d_frozen_nk) cudaFree(ctx->d_frozen_nk);

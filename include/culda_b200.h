@@ -580,6 +580,21 @@ int culda_mh_snapshot(culda_ctx *ctx, uint32_t iteration, int32_t steps, uint16_
  * sum to nk. */
 int culda_set_frozen_phi(culda_ctx *ctx, const int32_t *phi, const int32_t *nk);
 
+/* ------------------------------------ doc-chunk data parallelism (one rank per GPU)
+ * Replaces the phi exchange of -g N -c N (src_culda/train/MultiChunkMultiGPUequal.h:88-172,
+ * MasterGPUCollect/Reduce/Distribute in src_culda/model/model_phi.cpp:105-144).
+ * A context created on one chunk of the documents (a doc range, word ids of
+ * the whole vocabulary) writes its chunk's word-topic counts [V x K] and topic
+ * totals [K] of the current topics into caller-owned device buffers
+ * (culda_count_phi, synchronous); the caller sums those over the chunks in
+ * place (an all-reduce) and passes the sums to culda_set_shared_phi, after
+ * which the samplers read the word rows and totals from those buffers at
+ * every iteration (no copy; the caller keeps them alive and refreshed between
+ * iterations).  NULL buffers return the context to its own counts.  Theta and
+ * the topics stay the chunk's own. */
+int culda_count_phi(culda_ctx *ctx, int32_t *d_phi, int32_t *d_nk);
+int culda_set_shared_phi(culda_ctx *ctx, int32_t *d_phi, int32_t *d_nk);
+
 /* Warm start from the proposal set by culda_set_proposal: every token's topic
  * is drawn from q_d(k) * phihat_wk (Philox: seed, token, 0, 6), then the
  * counts are rebuilt. */

@@ -701,8 +701,13 @@ double oracle_loglik_reference(int32_t num_words, int32_t k, float alpha, int64_
                                const int32_t *slot_word, const int64_t *slot_range, const int32_t *doc_ids,
                                const int64_t *doc_ptr, const uint16_t *phi_head, const int16_t *theta_a,
                                const int16_t *theta_ja, const int32_t *max_ia, const int32_t *cur_ia) {
-    std::vector<float> cache((size_t)k), qtree(32);
     int64_t total = 0;
+    // slots are independent and the warp sums are integers after truncation,
+    // so the slots may run on all host threads in any order
+#pragma omp parallel reduction(+ : total)
+    {
+    std::vector<float> cache((size_t)k), qtree(32);
+#pragma omp for schedule(dynamic, 16)
     for (int32_t s = 0; s < num_slots; ++s) {
         const int32_t w = slot_word[s];
         for (int32_t j = 0; j < k; ++j) cache[j] = oracle_half_to_float(phi_head[(size_t)w * k + j]);
@@ -733,7 +738,48 @@ double oracle_loglik_reference(int32_t num_words, int32_t k, float alpha, int64_
             if (s < num_words) total += (int64_t)(int)(double)sum;
         }
     }
+    }
     return (double)total / (double)num_tokens;
+}
+
+/* The reference's slots (doc_chunk.cpp:148-205): words by length, longest
+ * first; a word longer than 1.05 * (N / 56) tokens is cut into
+ * ceil(len / ave) slices of ceil(len / slices) tokens.  The reference sorts
+ * with std::sort on the length alone, which leaves the order of words of equal
+ * length unspecified; here they keep ascending word id.  Writes num_slots
+ * (at most num_words + N / ave + 1) slot words and [start, end) ranges, and
+ * returns num_slots. */
+int32_t oracle_reference_slots(int32_t num_words, const int64_t *word_ptr, int32_t *slot_word, int64_t *slot_range) {
+    const int64_t n = word_ptr[num_words] - word_ptr[0];
+    const int ave = (int)(n / 56);
+    std::vector<int32_t> order((size_t)num_words);
+    for (int32_t w = 0; w < num_words; ++w) order[(size_t)w] = w;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return word_ptr[a + 1] - word_ptr[a] > word_ptr[b + 1] - word_ptr[b];
+    });
+    int32_t ns = 0;
+    for (int32_t w : order) {
+        const int len = (int)(word_ptr[w + 1] - word_ptr[w]);
+        if (ave > 0 && len > 1.05 * ave) {
+            const int slices = (len + ave - 1) / ave;
+            const int size = (len + slices - 1) / slices;
+            for (int i = 0; i < slices; ++i) {
+                const int64_t b = word_ptr[w] + (int64_t)size * i;
+                int64_t e = b + size;
+                if (e >= word_ptr[w + 1]) e = word_ptr[w + 1];
+                slot_word[ns] = w;
+                slot_range[2 * ns] = b;
+                slot_range[2 * ns + 1] = e;
+                ++ns;
+            }
+        } else {
+            slot_word[ns] = w;
+            slot_range[2 * ns] = word_ptr[w];
+            slot_range[2 * ns + 1] = word_ptr[w + 1];
+            ++ns;
+        }
+    }
+    return ns;
 }
 
 /* ------------------------------------------------------ joint likelihood */

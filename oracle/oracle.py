@@ -302,6 +302,20 @@ class RowSnapshot:
         return z_out, margin, ll_tok, (float(terms[0]), float(terms[1]))
 
 
+def reference_slots(word_ptr) -> tuple[np.ndarray, np.ndarray]:
+    """(slot_word, slot_range [slots x 2]): the reference's slots of a corpus
+    (oracle_reference_slots, doc_chunk.cpp:148-205)."""
+    wp = _c(word_ptr, np.int64)
+    v = len(wp) - 1
+    cap = v + 2 * 57 + 16  # slices of the long words add at most N / (N // 56) + 1 slots
+    sw = np.empty(cap, dtype=np.int32)
+    sr = np.empty(2 * cap, dtype=np.int64)
+    f = lib().oracle_reference_slots
+    f.restype = C.c_int32
+    ns = f(C.c_int32(v), _p(wp), _p(sw), _p(sr))
+    return sw[:ns].copy(), sr[:2 * ns].reshape(ns, 2).copy()
+
+
 def loglik_reference(snapshot: "Snapshot", num_tokens: int, slot_word, slot_range, phi_head_f16_table) -> float:
     """The log-likelihood the reference prints (oracle_loglik_reference)."""
     s = snapshot

@@ -113,3 +113,18 @@ def test_reference_draws_follow_the_conditional(fixture):
     own = stats.kstest(_pit(s, s.sample(7, 1)[0].astype(np.int64), head, 1), "uniform")
     assert own.pvalue > 0.01
     assert d_ref < 0.04
+
+
+def test_restated_slots_match_reference(fixture):
+    """oracle_reference_slots gives the reference's slots (doc_chunk.cpp:148-205):
+    the same (word, range) set in the same length order; words of equal length
+    may come in another order (the reference's std::sort leaves it open), which
+    moves the printed log-likelihood by at most a few truncation units."""
+    meta, f, c, s, _ = fixture
+    sw, sr = O.reference_slots(c.word_ptr)
+    gsw, gsr = f["slot_word"], f["slot_range"].reshape(-1, 2)
+    assert sorted(zip(sw.tolist(), map(tuple, sr.tolist()))) == sorted(zip(gsw.tolist(), map(tuple, gsr.tolist())))
+    assert np.array_equal(sr[:, 1] - sr[:, 0], gsr[:, 1] - gsr[:, 0])
+    head = O.phi_head_f16(s.num_words, s.k, s.beta, s.phi, s.nk)
+    ll = O.loglik_reference(s, c.num_tokens, sw, sr, head)
+    assert abs(ll - float(f["loglik"][0])) <= 4.0 / c.num_tokens

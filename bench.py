@@ -219,23 +219,56 @@ def workload(args, seed: int):
 # ----------------------------------------------- learned form and fold-in
 def measure_learned(args, wl, corpus, device) -> dict:
     """Wall-clock to the plain chain's iteration-100 log-likelihood, plain CGS
-    against the learned form: plain iterations 1-40 with states 21-40
-    accumulated, the encoder initialised from the word profiles and trained on
-    them, then Metropolis-Hastings iterations mixing the doc and encoder
-    proposals 1:1 (2 steps per token).  Every state's log-likelihood is the
-    per-token value of culda_sample_snapshot (evaluation passes are not
-    timed); iterations are timed with CUDA events, the host-driven steps
-    (accumulation, training, proposal tables) by the wall clock."""
+    against several schedules of the learned form.  Every state's
+    log-likelihood is the per-token value of culda_sample_snapshot (evaluation
+    passes are not timed); iterations are timed with CUDA events, the
+    host-driven steps (accumulation, training, proposal tables, warm start) by
+    the wall clock.
+
+    Schedules (each stops at the target or after its iteration budget):
+      mh2        plain 1-40 (states 21-40 accumulated), encoder initialised
+                 from the word profiles and trained, then MH iterations mixing
+                 the doc and encoder proposals 1:1, 2 steps per token;
+      mh8        the same trained state, 8 MH steps per token;
+      interleave the same trained state, then a plain sweep and a 2-step MH
+                 iteration in turn;
+      restart    plain 1-10 (states 6-10 accumulated), the encoder trained 2
+                 epochs, every topic redrawn from q_d(k) * phihat_wk (warm
+                 start), then plain sweeps.
+    The first three share the prefix (plain 1-40 and the training): its time
+    is counted in each, and each starts from the prefix's topics."""
     import culda_cgs_b200 as cb
 
-    target_it, first, window, epochs, max_mh = 100, 20, 20, args.learned_epochs, 60
+    target_it, first, window, epochs = 100, 20, 20, args.learned_epochs
     with cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device) as m:
         st = m.iterate(target_it)
         t_plain = sum(x["seconds"] for x in st)
         target = m.sample_snapshot(1 << 30)[1]
-        plain_curve = [(i + 1, round(sum(x["seconds"] for x in st[:i + 1]), 4)) for i in (39, 59, 79, 99)]
+        plain_curve = [(i + 1, round(sum(x["seconds"] for x in st[:i + 1]), 4)) for i in (9, 39, 59, 79, 99)]
     out = {"target": "log-likelihood per token of the plain chain's state after iteration 100",
            "target_loglik": round(target, 6), "plain_seconds": round(t_plain, 4), "plain_seconds_at": plain_curve}
+
+    def run(m, t, it, step, max_it, name):
+        curve, reached, secs, acc = [], None, [], []
+        while it < max_it:
+            sts = step(m)
+            it += len(sts)
+            t += sum(x["seconds"] for x in sts)
+            secs += [x["seconds"] for x in sts]
+            acc += [x["accept_rate"] for x in sts if x["accept_rate"] > 0]
+            ll = m.sample_snapshot(1 << 29)[1]
+            curve.append((it, round(t, 4), round(ll, 6)))
+            if ll >= target:
+                reached = t
+                break
+        return {"name": name, "reached": reached is not None,
+                "seconds_to_target": round(reached, 4) if reached else None,
+                "ratio_to_plain": round(reached / t_plain, 4) if reached else None,
+                "ms_per_iteration": round(1e3 * statistics.mean(secs), 4) if secs else None,
+                "mh_accept_rate": round(statistics.mean(acc), 4) if acc else None,
+                "last_loglik": curve[-1][2] if curve else None, "curve": curve[::max(1, len(curve) // 8)]}
+
+    schedules = []
     with cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device) as m, \
             cb.Encoder(corpus.num_words, wl.k, args.learned_batch, seed=1, device=device) as enc:
         t = sum(x["seconds"] for x in m.iterate(first))
@@ -250,30 +283,42 @@ def measure_learned(args, wl, corpus, device) -> dict:
         m.set_proposal(enc, mix=0.05)
         t_train = time.perf_counter() - t0
         t += t_train
-        curve, reached, accept, mh_sec = [], None, [], []
-        it = first + window
-        while it < first + window + max_mh:
-            st = m.iterate_mh(5, steps=2)
-            it += 5
-            t += sum(x["seconds"] for x in st)
-            mh_sec += [x["seconds"] for x in st]
-            accept += [x["accept_rate"] for x in st]
-            ll = m.sample_snapshot(1 << 29)[1]
-            curve.append((it, round(t, 4), round(ll, 6)))
-            if ll >= target:
-                reached = t
-                break
+        z_prefix, it_prefix = m.topics(), m.next_iteration()
+        out.update({"prefix": f"plain 1-{first + window} (states {first + 1}-{first + window} accumulated), "
+                              f"encoder trained {epochs} epochs (batch {args.learned_batch})",
+                    "prefix_seconds": round(t, 4), "encoder_train_seconds": round(t_train, 4),
+                    "encoder_loss": [round(losses[0], 4), round(losses[-1], 4)]})
+        budget = first + window + 60
+        for name, step in (("mh2", lambda mm: mm.iterate_mh(5, steps=2)),
+                           ("mh8", lambda mm: mm.iterate_mh(5, steps=8)),
+                           ("interleave", lambda mm: mm.iterate(1) + mm.iterate_mh(1, steps=2))):
+            m.set_topics(z_prefix)
+            m.set_iteration(it_prefix)
+            schedules.append(run(m, t, first + window, step, budget, name))
+    with cb.LDA(corpus, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device) as m, \
+            cb.Encoder(corpus.num_words, wl.k, args.learned_batch, seed=1, device=device) as enc:
+        t = sum(x["seconds"] for x in m.iterate(5))
+        for _ in range(5):
+            t += m.iterate(1)[0]["seconds"]
+            t0 = time.perf_counter()
+            m.accumulate_theta()
+            t += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        m.init_encoder(enc, seed=3)
+        for e in range(2):
+            m.train_encoder(enc, 1, seed=e)
+        m.set_proposal(enc, mix=0.05)
+        m.warm_start()
+        t += time.perf_counter() - t0
+        schedules.append(run(m, t, 10, lambda mm: mm.iterate(5), target_it + 20, "restart"))
+    best = min((x for x in schedules if x["reached"]), key=lambda x: x["seconds_to_target"], default=None)
     out.update({
-        "schedule": f"plain 1-{first + window} (states {first + 1}-{first + window} accumulated), encoder "
-                    f"initialised from word profiles and trained {epochs} epochs (batch {args.learned_batch}), then "
-                    f"MH doc:encoder 1:1, 2 steps per token, up to {max_mh} iterations",
-        "learned_seconds_to_target": round(reached, 4) if reached else None,
-        "reached": reached is not None,
-        "ratio_learned_to_plain": round(reached / t_plain, 4) if reached else None,
-        "encoder_train_seconds": round(t_train, 4), "encoder_loss": [round(losses[0], 4), round(losses[-1], 4)],
-        "mh_ms_per_iteration": round(1e3 * statistics.mean(mh_sec), 4) if mh_sec else None,
-        "mh_accept_rate": round(statistics.mean(accept), 4) if accept else None,
-        "learned_curve": curve})
+        "schedules": schedules,
+        "best_schedule": best["name"] if best else None,
+        "learned_seconds_to_target": best["seconds_to_target"] if best else None,
+        "reached": best is not None,
+        "ratio_learned_to_plain": best["ratio_to_plain"] if best else None,
+        "mh_ms_per_iteration": schedules[0]["ms_per_iteration"], "mh_accept_rate": schedules[0]["mh_accept_rate"]})
     return out
 
 

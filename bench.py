@@ -283,7 +283,7 @@ def measure_learned(args, wl, corpus, device) -> dict:
         m.set_proposal(enc, mix=0.05)
         t_train = time.perf_counter() - t0
         t += t_train
-        z_prefix, it_prefix = m.topics(), m.next_iteration()
+        z_prefix, it_prefix = m.topics(), m.next_iteration
         out.update({"prefix": f"plain 1-{first + window} (states {first + 1}-{first + window} accumulated), "
                               f"encoder trained {epochs} epochs (batch {args.learned_batch})",
                     "prefix_seconds": round(t, 4), "encoder_train_seconds": round(t_train, 4),
@@ -519,6 +519,7 @@ def run_ours(args, world, rank, local, pg):
         "variant": {"group_lanes": info["group_lanes"], "sample_blocks": info["sample_blocks"],
                     "token_order": "input" if args.no_reorder else "by doc length inside each word",
                     "autotuned": bool(info["tuned"]), "items": info["num_items"], "hot_words": info["num_hot"],
+                    "theta_min_len": info["theta_min_len"], "theta_long_docs": info["theta_long_docs"],
                     "resident_gb": round(info["device_bytes"] / 1e9, 3)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         "learned": learned, "foldin": foldin,

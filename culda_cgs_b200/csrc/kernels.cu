@@ -569,7 +569,7 @@ extern "C" int culda_sample(const culda_sample_args *a, void *d_workspace, size_
         workspace_bytes < culda_sample_workspace(a->k, a->num_items, a->num_hot) ||
         (a->group_lanes != kFlatLanes && a->group_lanes != 1 && a->group_lanes != 2 && a->group_lanes != 4 &&
          a->group_lanes != 8 && a->group_lanes != 16 && a->group_lanes != 32) ||
-        ((uintptr_t)a->theta & 15u)) {
+        ((uintptr_t)a->theta & 31u)) {
         set_global_error("culda_sample: invalid argument");
         return CULDA_ERR_INVALID_ARG;
     }

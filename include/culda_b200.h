@@ -32,8 +32,9 @@
  *                         topic inside a row, zero padded (reference: thetaA
  *                         and thetaJA, two int16 arrays,
  *                         lda_theta_kernel.cu:55-58).  The topic is kept as a
- *                         byte offset so the sampler needs one 16-byte load per
- *                         four entries and one shared-memory load per entry.
+ *                         byte offset so the sampler needs one 32-byte load per
+ *                         eight entries and one shared-memory load per entry;
+ *                         the array must be 32-byte aligned.
  *   theta_rows int32[2*D] {row start, row end} per doc; start is the reference's
  *                         thetaMaxIA[d], end its thetaCurIA[d] = start + roundup32(nnz)
  *   nk        int32[K]    tokens per topic (reference: phiTopic)
@@ -370,7 +371,7 @@ typedef struct culda_sample_args {
     const int32_t *doc_ids;      /* [N] */
     const uint16_t *topics_in;   /* [N] topics of the snapshot: phi rows are histogrammed from them */
     uint16_t *topics_out;        /* [N] sampled topics (must not alias topics_in) */
-    const uint32_t *theta;       /* packed CSR of the snapshot */
+    const uint32_t *theta;       /* packed CSR of the snapshot (32-byte aligned) */
     const int32_t *theta_rows;   /* [2*D] */
     const int32_t *nk;           /* [K] of the snapshot */
     const culda_item *items;     /* device copy of the work list (with segments) */
@@ -461,6 +462,10 @@ typedef struct culda_gemm_args {
     const float *pre;   /* [m x ldo] */
     float *colsum;      /* [n] */
     int32_t *error;     /* device int32 or NULL */
+    int32_t k_splits;   /* CULDA_GEMM_F32 only: 0 or 1 = one CTA per output tile; s > 1 cuts k
+                           into s slices whose partial products are added into out_f32 with
+                           atomics (out_f32 must hold zeros, or what to add to; bias is added
+                           once; the sum order, so the last bits, may vary run to run) */
 } culda_gemm_args;
 
 int culda_gemm_bf16(const culda_gemm_args *a, void *stream);

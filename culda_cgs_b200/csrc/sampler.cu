@@ -141,40 +141,11 @@ struct Step {
 // The 8 entries (32 bytes) at theta + idx in one 256-bit read-only load
 // (sm_100's ld.global.v8; theta is 32-byte aligned and idx a multiple of 8):
 // a group's step of 4 lanes is then one request per 128-byte line.
-#ifdef CULDA_L2_HINTS
-__device__ __forceinline__ void load8(const ThetaEntry *__restrict__ theta, int idx, uint32_t e[8]) {
-    asm("{\n\t.reg .b64 pol;\n\tcreatepolicy.fractional.L2::evict_last.b64 pol, 1.0;\n\t"
-        "ld.global.nc.L2::cache_hint.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], pol;\n\t}"
-        : "=r"(e[0]), "=r"(e[1]), "=r"(e[2]), "=r"(e[3]), "=r"(e[4]), "=r"(e[5]), "=r"(e[6]), "=r"(e[7])
-        : "l"(theta + idx));
-}
-template <class T>
-__device__ __forceinline__ T ld_stream(const T *p);
-template <>
-__device__ __forceinline__ float ld_stream<float>(const float *p) {
-    float v;
-    asm("{\n\t.reg .b64 pol;\n\tcreatepolicy.fractional.L2::evict_first.b64 pol, 1.0;\n\t"
-        "ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], pol;\n\t}" : "=f"(v) : "l"(p));
-    return v;
-}
-template <>
-__device__ __forceinline__ int ld_stream<int>(const int *p) {
-    int v;
-    asm("{\n\t.reg .b64 pol;\n\tcreatepolicy.fractional.L2::evict_first.b64 pol, 1.0;\n\t"
-        "ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], pol;\n\t}" : "=r"(v) : "l"(p));
-    return v;
-}
-#else
 __device__ __forceinline__ void load8(const ThetaEntry *__restrict__ theta, int idx, uint32_t e[8]) {
     asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
         : "=r"(e[0]), "=r"(e[1]), "=r"(e[2]), "=r"(e[3]), "=r"(e[4]), "=r"(e[5]), "=r"(e[6]), "=r"(e[7])
         : "l"(theta + idx));
 }
-template <class T>
-__device__ __forceinline__ T ld_stream(const T *p) {
-    return __ldg(p);
-}
-#endif
 
 __device__ __forceinline__ Step load_step(const ThetaEntry *__restrict__ theta, int idx, int re) {
     Step st;
@@ -651,12 +622,12 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
             int rs = 0, nu = 0, t0 = 0, tcount = 0;
             if (lane < nseg) {
                 const int sg = seg0 + lane;
-                const int64_t a0 = ld_stream(p.seg_start + sg);
-                const int64_t a1 = sg + 1 < sg_end ? (int64_t)ld_stream(p.seg_start + sg + 1) : iend;
+                const int64_t a0 = __ldg(p.seg_start + sg);
+                const int64_t a1 = sg + 1 < sg_end ? (int64_t)__ldg(p.seg_start + sg + 1) : iend;
                 if (a0 < ibeg || a1 > iend || a0 >= a1) {
                     atomicOr(p.error, kErrRowRange);
                 } else {
-                    const int d = ld_stream(p.doc_ids + a0);
+                    const int d = __ldg(p.doc_ids + a0);
                     if ((unsigned)d < (unsigned)p.num_docs) {
                         const int2 r = __ldg(p.rows + d);
                         if (r.x >= 0 && r.x <= r.y && (int64_t)r.y <= p.theta_cap && ((r.x | r.y) & 31) == 0 &&
@@ -783,7 +754,7 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
                     const int tok = m_t0[i] + (f - m_tc[i]);
                     float um;
                     if (p.uniforms) {
-                        um = ld_stream(p.uniforms + tok);
+                        um = __ldg(p.uniforms + tok);
                     } else {
                         const int64_t key = p.tok_index ? (int64_t)__ldg(p.tok_index + tok) : (int64_t)tok;
                         um = uniform_from_bits(philox_token(p.seed, (uint64_t)key, iter, kPurposeSample));

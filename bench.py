@@ -376,6 +376,32 @@ def common_config(wl, num_tokens: int, num_docs: int, num_words: int, seed: int,
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
+def measure_uneven(args, device) -> dict:
+    """The batched uneven workload (118M tokens, Pareto document lengths up
+    to 50k, V = 1M) at K = 1024 with the autotuner on: the sampler variant and
+    the theta rebuild's bin threshold it chose, and the iteration times after
+    tuning (iterations 4-8, CUDA events)."""
+    import culda_cgs_b200 as cb
+    from culda_cgs_b200.configs import UNEVEN
+
+    wl = UNEVEN.with_seed(args.seed)
+    c = cb.Corpus.generate(wl.gen)
+    with cb.LDA(c, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device, flags=cb.CULDA_FLAG_AUTOTUNE) as m:
+        m.iterate(3)  # the autotuner times the variants before iteration 3
+        st = m.iterate(5)
+        info = m.info()
+    sec = [x["seconds"] for x in st]
+    return {"workload": wl.name, "num_tokens": c.num_tokens, "num_docs": c.num_docs, "k": wl.k,
+            "autotuned": bool(info["tuned"]), "group_lanes": info["group_lanes"],
+            "sample_blocks": info["sample_blocks"], "theta_min_len": info["theta_min_len"],
+            "theta_long_docs": info["theta_long_docs"], "sampler_tune_ms": round(info["tune_ms"], 4),
+            "rebuild_tune_ms": round(info["theta_tune_ms"], 4),
+            "ms_per_iteration": round(1e3 * statistics.mean(sec), 4),
+            "sample_ms": round(1e3 * statistics.mean(x["sample_seconds"] for x in st), 4),
+            "rebuild_ms": round(1e3 * statistics.mean(x["rebuild_seconds"] for x in st), 4),
+            "tokens_per_sec": round(c.num_tokens / statistics.mean(sec), 1)}
+
+
 # ------------------------------------------------------------------- ours
 def run_ours(args, world, rank, local, pg):
     import ctypes as C
@@ -509,6 +535,12 @@ def run_ours(args, world, rank, local, pg):
             foldin = measure_foldin(args, local)
         except Exception as e:
             foldin = {"error": f"{type(e).__name__}: {e}"}
+    uneven = None
+    if rank == 0 and world == 1 and not args.no_uneven:
+        try:
+            uneven = measure_uneven(args, local)
+        except Exception as e:
+            uneven = {"error": f"{type(e).__name__}: {e}"}
 
     launches = info["kernels_per_iteration"] * args.steps
     line = {
@@ -522,10 +554,45 @@ def run_ours(args, world, rank, local, pg):
                     "theta_min_len": info["theta_min_len"], "theta_long_docs": info["theta_long_docs"],
                     "resident_gb": round(info["device_bytes"] / 1e9, 3)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
-        "learned": learned, "foldin": foldin,
+        "learned": learned, "foldin": foldin, "uneven": uneven,
         "loglik": [round(s["loglik"], 8) for s in stats],
     }
     return line
+
+
+# ------------------------------------------------------ encoder training
+def run_encoder(args, world, rank, local):
+    """--mode encoder: the learned proposal's encoder trained on the chain's
+    own states (plain iterations 1-40, states 21-40 accumulated), for each
+    batch size of --encoder-batches; prints seconds per epoch and the loss.
+    Rank 0 only."""
+    import torch
+
+    import culda_cgs_b200 as cb
+
+    if rank != 0:
+        return None
+    wl = workload(args, args.seed)
+    c = cb.Corpus.generate(wl.gen)
+    out = {"mode": "encoder", "config": common_config(wl, c.num_tokens, c.num_docs, c.num_words, args.seed, 1),
+           "epochs": args.learned_epochs, "runs": []}
+    with cb.LDA(c, wl.k, wl.alpha, wl.beta, seed=args.seed, device=local) as m:
+        m.iterate(20)
+        for _ in range(20):
+            m.iterate(1)
+            m.accumulate_theta()
+        for b in (int(x) for x in args.encoder_batches.split(",")):
+            with cb.Encoder(c.num_words, wl.k, b, seed=1, device=local) as enc:
+                m.init_encoder(enc, seed=3)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                losses = [m.train_encoder(enc, 1, seed=e) for e in range(args.learned_epochs)]
+                torch.cuda.synchronize()
+                t = time.perf_counter() - t0
+            out["runs"].append({"batch": b, "seconds": round(t, 4), "seconds_per_epoch": round(t / len(losses), 4),
+                                "docs_per_sec": round(c.num_docs * len(losses) / t, 1),
+                                "loss_first_last": [round(losses[0], 4), round(losses[-1], 4)]})
+    return out
 
 
 # ------------------------------------------------- doc-chunk data parallel
@@ -660,8 +727,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["replicas", "dp"], default="replicas",
-                    help="N > 1: independent replicas (default) or doc-chunk data parallelism")
+    ap.add_argument("--mode", choices=["replicas", "dp", "encoder"], default="replicas",
+                    help="N > 1: independent replicas (default) or doc-chunk data parallelism; "
+                         "encoder: time the learned proposal's training only")
+    ap.add_argument("--encoder-batches", default="1024,4096", help="--mode encoder: batch sizes")
     ap.add_argument("--workload", default="plain-cgs-scale")
     ap.add_argument("--k", type=int, default=0, help="topics (default: the workload's); alpha = 50/K")
     ap.add_argument("--seed", type=int, default=1)
@@ -676,6 +745,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work at most")
     ap.add_argument("--ref-timeout", type=float, default=1200.0)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-form and fold-in measurements")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the autotuned uneven-workload measurement")
     ap.add_argument("--learned-epochs", type=int, default=8)
     ap.add_argument("--learned-batch", type=int, default=1024)
     args = ap.parse_args()
@@ -688,6 +758,8 @@ def main():
             line = run_reference(args, world, rank)
         elif args.mode == "dp":
             line = run_dp(args, world, rank, local, pg)
+        elif args.mode == "encoder":
+            line = run_encoder(args, world, rank, local)
         else:
             line = run_ours(args, world, rank, local, pg)
         if rank == 0 and line is not None:

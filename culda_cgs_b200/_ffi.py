@@ -88,7 +88,7 @@ class GemmArgs(C.Structure):
     _fields_ = [("m", i32), ("n", i32), ("k", i32), ("a", C.c_void_p), ("lda", i32), ("b", C.c_void_p),
                 ("ldb", i32), ("epilogue", i32), ("alpha", f32), ("out_f32", C.c_void_p), ("out_bf16", C.c_void_p),
                 ("out_bf16_t", C.c_void_p), ("ldo", i32), ("ld_t", i32), ("bias", C.c_void_p), ("pre", C.c_void_p),
-                ("colsum", C.c_void_p), ("error", C.c_void_p)]
+                ("colsum", C.c_void_p), ("error", C.c_void_p), ("k_splits", i32)]
 
 
 CULDA_ENC_EMBED, CULDA_ENC_HIDDEN = 256, 512

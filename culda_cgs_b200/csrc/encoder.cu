@@ -14,12 +14,16 @@
 //             dP2 = (dZ W3) * GELU'(P2)              GEMM(dZ, W3^T), db2 = column sums
 //             dW2 = dP2^T H1,  dP1 = (dP2 W2) * GELU'(P1), db1
 //             dW1 = dP1^T X0,  dX0 = dP1 W1          FP32
-//             dE[w] += dX0[b] / L_b for every token of doc b
-// Every GEMM is C = A B^T with both operands K-major, so each weight is kept
+//             dE[w] = sum of dX0[b] / L_b over the tokens of w in the batch
+//                   (tokens grouped by word, one write per embedding row)
+// The weight gradients split their K range (the batch) over several CTAs
+// per tile.  Every GEMM is C = A B^T with both operands K-major, so each weight is kept
 // in BF16 twice (W and W^T) and each activation that feeds a weight gradient
 // is written transposed by the epilogue that produces it.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -112,46 +116,103 @@ __global__ void embbag_fwd_kernel(int batch, int rows, const int32_t *__restrict
     }
 }
 
-// dE[w] += dX0[b] / L_b for every token of row b (vector atomics).
-__global__ void embbag_bwd_kernel(int batch, const int32_t *__restrict__ docs, const int64_t *__restrict__ doc_ptr,
-                                  const int32_t *__restrict__ words, int V, const float *__restrict__ dX0, float *gE) {
+// The embedding gradient: the batch's tokens are grouped by word (a counting
+// sort: counts per word, their exclusive scan, placement), the grouped list
+// is cut into chunks of 32 tokens, and a warp walks its chunk in order,
+// summing dX0[b] / L_b per word in registers.  A word whose tokens all lie in
+// the chunk is written with plain stores; a word spread over several chunks
+// (the frequent ones) adds each chunk's partial sum with one vector atomic
+// per lane.  gE holds zeros before the pass.
+
+// cnt[w] += 1 for every token of batch row b (warp per row); inv_len[b] = 1 / L_b.
+__global__ void bag_count_kernel(int batch, const int32_t *__restrict__ docs, const int64_t *__restrict__ doc_ptr,
+                                 const int32_t *__restrict__ words, int V, int32_t *cnt, float *inv_len,
+                                 unsigned long long *total) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < batch; b += nw) {
         const int d = docs ? docs[b] : b;
         const int64_t t0 = doc_ptr[d], t1 = doc_ptr[d + 1];
-        if (t1 <= t0) continue;
-        const float inv = 1.0f / (float)(t1 - t0);
-        const float4 *src = reinterpret_cast<const float4 *>(dX0 + (size_t)b * kE) + 2 * lane;
-        float4 g0 = src[0], g1 = src[1];
-        g0 = make_float4(g0.x * inv, g0.y * inv, g0.z * inv, g0.w * inv);
-        g1 = make_float4(g1.x * inv, g1.y * inv, g1.z * inv, g1.w * inv);
-        // runs of one word (a document's words arrive sorted when the CSR is
-        // the doc-ordered token list) are added with one atomic per column
-        int run_w = -1;
-        float mult = 0.f;
-        auto flush = [&]() {
-            if (run_w < 0) return;
-            float4 *dst = reinterpret_cast<float4 *>(gE + (size_t)run_w * kE) + 2 * lane;
-            atomicAdd(dst, make_float4(g0.x * mult, g0.y * mult, g0.z * mult, g0.w * mult));
-            atomicAdd(dst + 1, make_float4(g1.x * mult, g1.y * mult, g1.z * mult, g1.w * mult));
-        };
-        for (int64_t tb = t0; tb < t1; tb += 32) {
-            const int wl = tb + lane < t1 ? words[tb + lane] : 0;
-            const int n = (int)min((int64_t)32, t1 - tb);
-            for (int j = 0; j < n; ++j) {
-                const int w = __shfl_sync(0xffffffffu, wl, j);
-                if ((unsigned)w >= (unsigned)V) continue;  // reported by the forward pass
-                if (w == run_w) {
-                    mult += 1.f;
-                } else {
-                    flush();
-                    run_w = w;
-                    mult = 1.f;
-                }
+        int n = 0;
+        for (int64_t t = t0 + lane; t < t1; t += 32) {
+            const int w = words[t];
+            if ((unsigned)w < (unsigned)V) {
+                atomicAdd(&cnt[w], 1);
+                ++n;
             }
         }
-        flush();
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+        if (lane == 0) {
+            inv_len[b] = t1 > t0 ? 1.0f / (float)(t1 - t0) : 0.f;
+            if (total) atomicAdd(total, (unsigned long long)n);
+        }
+    }
+}
+
+// rows[start[w] + fill[w]++] = b and wid[...] = w for every token of batch row b.
+__global__ void bag_place_kernel(int batch, const int32_t *__restrict__ docs, const int64_t *__restrict__ doc_ptr,
+                                 const int32_t *__restrict__ words, int V, const int32_t *__restrict__ start,
+                                 int32_t *fill, int32_t *rows, int32_t *wid) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < batch; b += nw) {
+        const int d = docs ? docs[b] : b;
+        const int64_t t0 = doc_ptr[d], t1 = doc_ptr[d + 1];
+        for (int64_t t = t0 + lane; t < t1; t += 32) {
+            const int w = words[t];
+            if ((unsigned)w < (unsigned)V) {
+                const int pos = start[w] + atomicAdd(&fill[w], 1);
+                rows[pos] = b;
+                wid[pos] = w;
+            }
+        }
+    }
+}
+
+// Warp per chunk of 32 grouped tokens; each lane holds 8 of the 256 columns.
+// The grouped list holds start[V] tokens (those with a word id below V).
+__global__ void embbag_bwd_grouped_kernel(int V, const int32_t *__restrict__ start,
+                                          const int32_t *__restrict__ rows, const int32_t *__restrict__ wid,
+                                          const float *__restrict__ inv_len, const float *__restrict__ dX0,
+                                          float *gE) {
+    const int64_t n = start[V];
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; c0 < n; c0 += nw * 32) {
+        const int cn = (int)min((int64_t)32, n - c0);
+        const int my_w = lane < cn ? wid[c0 + lane] : -1;
+        const int my_b = lane < cn ? rows[c0 + lane] : 0;
+        const float my_s = lane < cn ? inv_len[my_b] : 0.f;
+        float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
+        for (int j = 0; j < cn; ++j) {
+            const int w = __shfl_sync(0xffffffffu, my_w, j);
+            const int b = __shfl_sync(0xffffffffu, my_b, j);
+            const float sc = __shfl_sync(0xffffffffu, my_s, j);
+            const float4 *src = reinterpret_cast<const float4 *>(dX0 + (size_t)b * kE) + 2 * lane;
+            const float4 g0 = src[0], g1 = src[1];
+            a0.x += g0.x * sc;
+            a0.y += g0.y * sc;
+            a0.z += g0.z * sc;
+            a0.w += g0.w * sc;
+            a1.x += g1.x * sc;
+            a1.y += g1.y * sc;
+            a1.z += g1.z * sc;
+            a1.w += g1.w * sc;
+            const int wn = __shfl_sync(0xffffffffu, my_w, (j + 1) & 31);
+            if (j + 1 == cn || wn != w) {  // the end of this word's run in the chunk
+                float4 *dst = reinterpret_cast<float4 *>(gE + (size_t)w * kE) + 2 * lane;
+                if (start[w] >= c0 && start[w + 1] <= c0 + cn) {  // the whole word: no other chunk adds to it
+                    dst[0] = a0;
+                    dst[1] = a1;
+                } else {
+                    atomicAdd(dst, a0);
+                    atomicAdd(dst + 1, a1);
+                }
+                a0 = make_float4(0.f, 0.f, 0.f, 0.f);
+                a1 = a0;
+            }
+        }
     }
 }
 
@@ -251,6 +312,15 @@ struct culda_encoder {
     float *P1 = nullptr, *P2 = nullptr, *Z = nullptr, *dX0 = nullptr;
     double *d_loss = nullptr;
     int32_t *d_error = nullptr;
+    // the batch's tokens grouped by word for the embedding gradient
+    int32_t *bag_cnt = nullptr, *bag_start = nullptr;  // [V + 1] each
+    int32_t *bag_rows = nullptr;                        // [bag_cap] batch row of every token, by word
+    int32_t *bag_wid = nullptr;                         // [bag_cap] its word
+    int64_t bag_cap = 0;
+    float *bag_inv_len = nullptr;                       // [Bmax] 1 / L of every batch row
+    unsigned long long *bag_total = nullptr;            // tokens of the batch (device)
+    void *scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
     std::vector<void *> allocs;
 
     float *tensor(int t) { return params + off[t]; }
@@ -306,6 +376,20 @@ cudaError_t gemm(int M, int N, int K, const bf16 *A, const bf16 *B, int epi, con
     return gemm_bf16_nt(M, N, K, A, K, B, K, epi, ep, err, s);
 }
 
+// Weight gradients: M x N is a few tiles and K the batch, so the K range is
+// cut into slices (at least 4 k-blocks each) until about two CTAs per SM are
+// busy; the slices add into the zeroed gradient.
+cudaError_t gemm_wgrad(int M, int N, int K, const bf16 *A, const bf16 *B, GemmEpilogue ep, int32_t *err,
+                       cudaStream_t s) {
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (M / 128) * (N / 128);
+    const int by_k = std::max(1, (K / 64) / 4);
+    ep.k_splits = std::max(1, std::min(by_k, (2 * sms + tiles - 1) / tiles));
+    return gemm_bf16_nt(M, N, K, A, K, B, K, kEpiF32, ep, err, s);
+}
+
 }  // namespace
 
 int encoder_k(const culda_encoder *e) { return e->K; }
@@ -319,7 +403,7 @@ int encoder_max_batch(const culda_encoder *e) { return e->Bmax; }
 int32_t *encoder_error_word(culda_encoder *e) { return e->d_error; }
 
 int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t *doc_ptr, const int32_t *words,
-                 const EncoderTarget *target, bool update, float *probs, cudaStream_t s) {
+                 const EncoderTarget *target, bool update, float *probs, cudaStream_t s, int64_t batch_tokens) {
     if (batch <= 0 || batch > e->Bmax || !doc_ptr || !words)
         return fail_enc(CULDA_ERR_INVALID_ARG, "encoder: %s", "batch outside 1..max_batch or null CSR");
     if (target && !target->dense && !target->acc)
@@ -366,7 +450,7 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
     GemmEpilogue gw;
     gw.ldo = kH;
     gw.out_f32 = e->grad(CULDA_ENC_W3);
-    ECK(gemm(K, kH, Bp, e->dZt, e->H2t, kEpiF32, gw, err, s));  // dW3 = dZ^T H2
+    ECK(gemm_wgrad(K, kH, Bp, e->dZt, e->H2t, gw, err, s));  // dW3 = dZ^T H2
     GemmEpilogue gb;
     gb.ldo = kH;
     gb.ld_t = Bp;
@@ -376,7 +460,7 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
     gb.colsum = e->grad(CULDA_ENC_B2);
     ECK(gemm(Bp, kH, K, e->dZ, e->W3t, kEpiGeluBwd, gb, err, s));  // dP2 = (dZ W3) GELU'(P2)
     gw.out_f32 = e->grad(CULDA_ENC_W2);
-    ECK(gemm(kH, kH, Bp, e->dP2t, e->H1t, kEpiF32, gw, err, s));  // dW2 = dP2^T H1
+    ECK(gemm_wgrad(kH, kH, Bp, e->dP2t, e->H1t, gw, err, s));  // dW2 = dP2^T H1
     gb.pre = e->P1;
     gb.out_bf16 = e->dP1;
     gb.out_bf16_t = e->dP1t;
@@ -385,12 +469,48 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
     GemmEpilogue g1;
     g1.ldo = kE;
     g1.out_f32 = e->grad(CULDA_ENC_W1);
-    ECK(gemm(kH, kE, Bp, e->dP1t, e->X0t, kEpiF32, g1, err, s));  // dW1 = dP1^T X0
+    ECK(gemm_wgrad(kH, kE, Bp, e->dP1t, e->X0t, g1, err, s));  // dW1 = dP1^T X0
     g1.out_f32 = e->dX0;
     ECK(gemm(Bp, kE, kH, e->dP1, e->W1t, kEpiF32, g1, err, s));  // dX0 = dP1 W1
-    embbag_bwd_kernel<<<grid_for((int64_t)batch * 32), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->dX0,
-                                                                    e->grad(CULDA_ENC_E));
+    // the batch's tokens grouped by word, then one write of every embedding row's gradient
+    const size_t vb = sizeof(int32_t) * ((size_t)e->V + 1);
+    ECK(cudaMemsetAsync(e->bag_cnt, 0, vb, s));
+    if (batch_tokens < 0) ECK(cudaMemsetAsync(e->bag_total, 0, sizeof(unsigned long long), s));
+    bag_count_kernel<<<grid_for((int64_t)batch * 32), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_cnt,
+                                                                   e->bag_inv_len,
+                                                                   batch_tokens < 0 ? e->bag_total : nullptr);
     ECK(cudaGetLastError());
+    if (batch_tokens < 0) {
+        unsigned long long n = 0;
+        ECK(cudaMemcpyAsync(&n, e->bag_total, sizeof n, cudaMemcpyDeviceToHost, s));
+        ECK(cudaStreamSynchronize(s));
+        batch_tokens = (int64_t)n;
+    }
+    if (batch_tokens > e->bag_cap) {
+        ECK(cudaStreamSynchronize(s));
+        for (int32_t **q : {&e->bag_rows, &e->bag_wid}) {
+            if (*q) {
+                cudaFree(*q);
+                e->allocs.erase(std::find(e->allocs.begin(), e->allocs.end(), (void *)*q));
+                *q = nullptr;
+            }
+        }
+        const int64_t cap = std::max<int64_t>(batch_tokens, 2 * e->bag_cap);
+        ECK(ealloc(e, &e->bag_rows, (size_t)cap));
+        ECK(ealloc(e, &e->bag_wid, (size_t)cap));
+        e->bag_cap = cap;
+    }
+    ECK(cub::DeviceScan::ExclusiveSum(e->scan_tmp, e->scan_tmp_bytes, e->bag_cnt, e->bag_start, e->V + 1, s));
+    ECK(cudaMemsetAsync(e->bag_cnt, 0, vb, s));
+    bag_place_kernel<<<grid_for((int64_t)batch * 32), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_start,
+                                                                   e->bag_cnt, e->bag_rows, e->bag_wid);
+    ECK(cudaGetLastError());
+    if (batch_tokens > 0) {
+        embbag_bwd_grouped_kernel<<<grid_for(batch_tokens), 256, 0, s>>>(e->V, e->bag_start, e->bag_rows,
+                                                                         e->bag_wid, e->bag_inv_len, e->dX0,
+                                                                         e->grad(CULDA_ENC_E));
+        ECK(cudaGetLastError());
+    }
     if (update) {
         e->steps += 1;
         const float c1 = 1.0f / (1.0f - powf(e->b1, (float)e->steps));
@@ -439,6 +559,7 @@ extern "C" int culda_gemm_bf16(const culda_gemm_args *a, void *stream) {
     ep.pre = a->pre;
     ep.colsum = a->colsum;
     ep.alpha = a->alpha;
+    ep.k_splits = a->k_splits > 0 ? a->k_splits : 1;
     if (const char *why = gemm_check(a->m, a->n, a->k, a->a, a->lda, a->b, a->ldb, a->epilogue, ep)) {
         set_global_error("culda_gemm_bf16: %s", why);
         return CULDA_ERR_INVALID_ARG;
@@ -517,6 +638,17 @@ extern "C" int culda_encoder_create(const culda_encoder_params *p, culda_encoder
     EALLOC(e->dX0, B * kE);
     EALLOC(e->d_loss, 1);
     EALLOC(e->d_error, 1);
+    EALLOC(e->bag_cnt, (size_t)e->V + 1);
+    EALLOC(e->bag_start, (size_t)e->V + 1);
+    EALLOC(e->bag_inv_len, B);
+    EALLOC(e->bag_total, 1);
+    r = cub::DeviceScan::ExclusiveSum(nullptr, e->scan_tmp_bytes, e->bag_cnt, e->bag_start, e->V + 1);
+    if (r != cudaSuccess) return bail(r);
+    {
+        uint8_t *tmp = nullptr;
+        EALLOC(tmp, e->scan_tmp_bytes);
+        e->scan_tmp = tmp;
+    }
 #undef EALLOC
     cudaStream_t s = nullptr;
     r = cudaMemsetAsync(e->grads, 0, sizeof(float) * np, s);

@@ -20,9 +20,11 @@ struct EncoderTarget {
 };
 
 // One forward (+ backward, + Adam step) pass; probs (optional) receives q.
+// batch_tokens is the batch's token count when the caller knows it, else -1
+// (the backward pass then counts it on the device and reads it back).
 // Returns a CULDA status; the loss is summed on the device into *d_loss.
 int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t *doc_ptr, const int32_t *words,
-                 const EncoderTarget *target, bool update, float *probs, cudaStream_t s);
+                 const EncoderTarget *target, bool update, float *probs, cudaStream_t s, int64_t batch_tokens = -1);
 
 // Mean cross-entropy of the passes since the last call (synchronises s).
 int encoder_take_loss(culda_encoder *e, int batch_rows, double *loss, cudaStream_t s);

@@ -5,8 +5,10 @@
 // stored in BF16 both as is and transposed), and the GELU backward (times
 // GELU'(pre), BF16 out and transposed, bias-gradient column sums).
 //
-// One CTA of 128 threads per 128 x 128 output tile.  Warp 0 lane 0 streams
-// 128 x 64 tiles of A and B into a 4-stage shared-memory ring with TMA
+// One CTA of 128 threads per 128 x 128 output tile (and per K slice when the
+// K range is split), two CTAs resident per SM so one tile's epilogue runs
+// while the other's MMAs do.  Warp 0 lane 0 streams
+// 128 x 64 tiles of A and B into a 3-stage shared-memory ring with TMA
 // (128-byte swizzle); warp 1 lane 0 issues tcgen05.mma (M = 128, N = 128,
 // K = 16 per instruction) into 128 TMEM columns and frees each stage with
 // tcgen05.commit; when the last MMA has landed all four warps read their 32
@@ -27,7 +29,7 @@ namespace culda {
 
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64, kStages = 4;
+constexpr int kBM = 128, kBN = 128, kBK = 64, kStages = 3;
 constexpr int kTileBytes = kBM * kBK * 2;  // 16 KB; the B tile (kBN rows) is the same size
 constexpr int kGemmThreads = 128;
 constexpr size_t kGemmSmem = (size_t)kStages * 2 * kTileBytes + 1024;  // + alignment slack
@@ -54,11 +56,17 @@ template <int EPI>
 __device__ __forceinline__ void epilogue(const GemmEpilogue &ep, int row, int col, float v[16], int lane) {
     const size_t o = (size_t)row * ep.ldo + col;
     if constexpr (EPI == kEpiF32) {
+        const bool with_bias = ep.bias && blockIdx.z == 0;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = v[i] * ep.alpha + (ep.bias ? ep.bias[col + i] : 0.f);
+        for (int i = 0; i < 16; ++i) v[i] = v[i] * ep.alpha + (with_bias ? ep.bias[col + i] : 0.f);
         float4 *d = reinterpret_cast<float4 *>(ep.out_f32 + o);
+        if (ep.k_splits > 1) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            for (int i = 0; i < 4; ++i) atomicAdd(d + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        }
     } else if constexpr (EPI == kEpiBiasGelu) {
         float4 *pre = reinterpret_cast<float4 *>(ep.out_f32 + o);
 #pragma unroll
@@ -96,7 +104,7 @@ __device__ __forceinline__ void epilogue(const GemmEpilogue &ep, int row, int co
 }
 
 template <int EPI>
-__global__ void __launch_bounds__(kGemmThreads, 1)
+__global__ void __launch_bounds__(kGemmThreads, 2)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b, int K,
                      const GemmEpilogue ep, int32_t *error) {
     extern __shared__ uint8_t gsm_raw[];
@@ -108,7 +116,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     uint8_t *base = gsm_raw + ((1024u - (raw & 1023u)) & 1023u);  // 1024-byte aligned for the swizzle
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-    const int nk = K / kBK;
+    // this CTA's K slice: k-blocks [kb0, kb0 + nk)
+    const int nk_all = K / kBK;
+    const int kb0 = (int)(((int64_t)nk_all * blockIdx.z) / gridDim.z);
+    const int nk = (int)(((int64_t)nk_all * (blockIdx.z + 1)) / gridDim.z) - kb0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -140,8 +151,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                     break;
                 }
                 umma::mbar_arrive_expect_tx(&full[s], 2u * kTileBytes);
-                umma::tma_load_2d(base + (size_t)s * kTileBytes, &tma_a, kb * kBK, m0, &full[s]);
-                umma::tma_load_2d(base + (size_t)(kStages + s) * kTileBytes, &tma_b, kb * kBK, n0, &full[s]);
+                umma::tma_load_2d(base + (size_t)s * kTileBytes, &tma_a, (kb0 + kb) * kBK, m0, &full[s]);
+                umma::tma_load_2d(base + (size_t)(kStages + s) * kTileBytes, &tma_b, (kb0 + kb) * kBK, n0, &full[s]);
             }
         }
         __syncwarp();
@@ -230,7 +241,7 @@ cudaError_t launch(const CUtensorMap &a, const CUtensorMap &b, int M, int N, int
                                     (int)kGemmSmem);
     });
     if (attr != cudaSuccess) return attr;
-    gemm_bf16_kernel<EPI><<<dim3(N / kBN, M / kBM), kGemmThreads, kGemmSmem, s>>>(a, b, K, ep, error);
+    gemm_bf16_kernel<EPI><<<dim3(N / kBN, M / kBM, ep.k_splits), kGemmThreads, kGemmSmem, s>>>(a, b, K, ep, error);
     return cudaGetLastError();
 }
 
@@ -244,6 +255,8 @@ const char *gemm_check(int M, int N, int K, const void *A, int lda, const void *
     if (!A || !B || !aligned16(A) || !aligned16(B)) return "A and B must be 16-byte aligned device pointers";
     if (lda < K || ldb < K || lda % 8 || ldb % 8) return "lda, ldb must be >= K and multiples of 8";
     if (ep.ldo < N || ep.ldo % 4) return "ldo must be >= N and a multiple of 4";
+    if (ep.k_splits < 1 || ep.k_splits > K / kBK) return "k_splits must be in 1..K/64";
+    if (ep.k_splits > 1 && epi != kEpiF32) return "split-K needs the F32 epilogue";
     switch (epi) {
         case kEpiF32:
             if (!ep.out_f32 || !aligned16(ep.out_f32)) return "F32 epilogue needs a 16-byte aligned out_f32";

@@ -24,6 +24,10 @@ struct GemmEpilogue {
     const float *pre = nullptr;
     float *colsum = nullptr;
     float alpha = 1.0f;
+    // split-K (kEpiF32 only): the K range is cut into k_splits CTAs per tile,
+    // each adding its partial product into out_f32 with atomics (out_f32 must
+    // hold zeros, or the value to add to, before the launch; bias is added once)
+    int k_splits = 1;
 };
 
 // nullptr when the shapes, strides and pointers are acceptable, else why not.

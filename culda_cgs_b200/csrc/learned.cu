@@ -559,9 +559,12 @@ extern "C" int culda_train_encoder(culda_ctx *ctx, culda_encoder *enc, int32_t e
         // batches of B docs; the last one holds the remainder
         const int steps = (ctx->D + B - 1) / B;
         for (int st = 0; st < steps && rc == CULDA_OK; ++st) {
-            const int b0 = st * B;
-            rc = encoder_pass(enc, std::min(B, ctx->D - b0), d_order + b0, ctx->d_doc_ptr, ctx->d_doc_words, &tg,
-                              true, nullptr, s);
+            const int b0 = st * B, nb = std::min(B, ctx->D - b0);
+            int64_t tokens = 0;  // the batch's tokens, known here from the host doc index
+            for (int i = b0; i < b0 + nb; ++i)
+                tokens += ctx->h_doc_ptr[(size_t)order[(size_t)i] + 1] - ctx->h_doc_ptr[(size_t)order[(size_t)i]];
+            rc = encoder_pass(enc, nb, d_order + b0, ctx->d_doc_ptr, ctx->d_doc_words, &tg, true, nullptr, s,
+                              tokens);
         }
         if (rc == CULDA_OK) rc = encoder_take_loss(enc, ctx->D, &last, s);
         if (rc) fail(ctx, rc, "culda_train_encoder: %s", global_error());

@@ -530,6 +530,38 @@ __device__ __forceinline__ int row_last_nonzero(const ThetaEntry *__restrict__ t
     return last;
 }
 
+// Items of at most kTinyTokens tokens (the long tail of the vocabulary) do not
+// rebuild the K-wide phihat row and dense prefix: a CTA keeps the row of a word
+// with no tokens, phihat_k = beta / (n_k + V beta), and its dense prefix, and an
+// item only writes its own (at most 32) topics' phihat, the same values a full
+// build gives, and restores them afterwards.  The dense prefix of the word is
+// the base prefix plus the cumulative corrections alpha * (phihat_wk - base_k)
+// of its topics, applied during the search.
+constexpr int kTinyTokens = 32;
+
+// First topic whose corrected dense prefix qc[j] + D(j) exceeds tq (K-1 when
+// none does); D(j) = dcum[i] for the last of the word's sorted topics tk[i] <= j.
+__device__ __forceinline__ int dense_search_tiny(const float *qc, int K, float tq, const int *tk, const float *dcum,
+                                                 int m) {
+    int lo = 0, hi = K - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        int a = 0, b = m;  // topics of the word up to mid
+        while (a < b) {
+            const int c = (a + b) >> 1;
+            if (tk[c] <= mid)
+                a = c + 1;
+            else
+                b = c;
+        }
+        if (fsum(qc[mid], a > 0 ? dcum[a - 1] : 0.f) > tq)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return lo;
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const SampleParams p) {
     extern __shared__ float smem[];
@@ -540,6 +572,11 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
     __shared__ int s_item, s_chunk;
     __shared__ float s_warp[kSampleThreads / 32];
     __shared__ double s_red[kSampleThreads / 32];
+    // tiny items: whether ph / qc hold the base row, and the item's topics
+    __shared__ int s_tiny, s_tm;
+    __shared__ int s_tk[kTinyTokens];
+    __shared__ float s_tdc[kTinyTokens];
+    __shared__ float s_tQ;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wl = lane & (kWalkLanes - 1), wg = lane / kWalkLanes;  // lane in its walk group, group
@@ -554,6 +591,7 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
     const uint32_t iter = p.iteration_ptr ? *p.iteration_ptr : p.iteration;
 
     for (int j = K + tid; j < KP; j += blockDim.x) ph[j] = 0.f;
+    if (tid == 0) s_tiny = 0;
 
     for (;;) {
         if (tid == 0) {
@@ -576,33 +614,90 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
         }
 
         // phi row of the word
-        const int *src;
-        if (p.frozen_phi) {
-            src = p.frozen_phi + (size_t)item.word * K;
-        } else if (item.hot < 0) {
-            for (int j = tid; j < K; j += blockDim.x) hist[j] = 0;
-            __syncthreads();
-            for (int64_t t = ibeg + tid; t < iend; t += blockDim.x) {
-                const uint32_t z = p.topics_in[t];
-                if (z < (uint32_t)K)
-                    atomicAdd(&hist[z], 1);
-                else
-                    atomicOr(p.error, kErrTopicRange);
+        const bool tiny = !p.frozen_phi && item.hot < 0 && item.count <= kTinyTokens;
+        float Q;
+        if (tiny) {
+            if (!s_tiny) {  // the base row and its dense prefix, once per CTA
+                for (int j = tid; j < K; j += blockDim.x)
+                    ph[j] = (0.f + p.beta) * (1.0f / ((float)__ldg(p.nk + j) + p.vbeta));
+                __syncthreads();
+                dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
+                __syncthreads();
+                if (tid == 0) s_tiny = 1;
+            }
+            if (warp == 0) {
+                // the item's distinct topics (match groups), their counts and ranks
+                uint32_t z = 0xFFFFFFFFu;
+                if (lane < (int)item.count) {
+                    z = p.topics_in[ibeg + lane];
+                    if (z >= (uint32_t)K) {
+                        atomicOr(p.error, kErrTopicRange);
+                        z = 0xFFFFFFFFu;
+                    }
+                }
+                const unsigned grp = __match_any_sync(0xffffffffu, z);
+                const bool lead = z != 0xFFFFFFFFu && __ffs(grp) - 1 == lane;
+                const uint32_t key = lead ? z : 0xFFFFFFFFu;
+                int rank = 0;
+#pragma unroll 8
+                for (int j = 0; j < 32; ++j) rank += __shfl_sync(0xffffffffu, key, j) < key;
+                const int m = __popc(__ballot_sync(0xffffffffu, lead));
+                float d = 0.f;
+                if (lead) {
+                    const float v = ((float)__popc(grp) + p.beta) * (1.0f / ((float)__ldg(p.nk + z) + p.vbeta));
+                    d = p.alpha * v - p.alpha * ph[z];  // ph[z] holds the base value here
+                    ph[z] = v;
+                    s_tk[rank] = (int)z;
+                    s_tdc[rank] = d;
+                }
+                // the corrections in topic order, then their running sums
+                __syncwarp();
+                float dc = lane < m ? s_tdc[lane] : 0.f;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const float t = __shfl_up_sync(0xffffffffu, dc, o);
+                    if (lane >= o) dc = fsum(dc, t);
+                }
+                __syncwarp();
+                if (lane < m) s_tdc[lane] = dc;
+                const float total = __shfl_sync(0xffffffffu, dc, m > 0 ? m - 1 : 0);
+                if (lane == 0) {
+                    s_tm = m;
+                    s_tQ = fsum(qc[K - 1], m > 0 ? total : 0.f);
+                }
             }
             __syncthreads();
-            src = hist;
+            Q = s_tQ;
         } else {
-            src = p.hot_phi + (size_t)item.hot * K;
+            const int *src;
+            if (p.frozen_phi) {
+                src = p.frozen_phi + (size_t)item.word * K;
+            } else if (item.hot < 0) {
+                for (int j = tid; j < K; j += blockDim.x) hist[j] = 0;
+                __syncthreads();
+                for (int64_t t = ibeg + tid; t < iend; t += blockDim.x) {
+                    const uint32_t z = p.topics_in[t];
+                    if (z < (uint32_t)K)
+                        atomicAdd(&hist[z], 1);
+                    else
+                        atomicOr(p.error, kErrTopicRange);
+                }
+                __syncthreads();
+                src = hist;
+            } else {
+                src = p.hot_phi + (size_t)item.hot * K;
+            }
+            // 1 / (n_k + V beta) is formed per item (the same operations, so the
+            // same bits, as a table would hold): without the table's 4 KB the
+            // 48-register build fits 10 CTAs per SM
+            for (int j = tid; j < K; j += blockDim.x)
+                ph[j] = ((float)src[j] + p.beta) * (1.0f / ((float)__ldg(p.nk + j) + p.vbeta));
+            __syncthreads();
+            dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
+            __syncthreads();
+            Q = qc[K - 1];
+            if (tid == 0) s_tiny = 0;  // read by every thread before the barrier above
         }
-        // 1 / (n_k + V beta) is formed per item (the same operations, so the
-        // same bits, as a table would hold): without the table's 4 KB the
-        // 48-register build fits 10 CTAs per SM
-        for (int j = tid; j < K; j += blockDim.x)
-            ph[j] = ((float)src[j] + p.beta) * (1.0f / ((float)__ldg(p.nk + j) + p.vbeta));
-        __syncthreads();
-        dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
-        __syncthreads();
-        const float Q = qc[K - 1];
 
         double ll = 0.0;
         const int sg_end = item.seg_begin + item.seg_count;
@@ -779,7 +874,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
                         // one unit in the last place above the previous unit's prefix)
                         if (z < 0) z = row_last_nonzero(p.theta, m_rs[i], m_rs[i] + kUnit * (m_cum[i + 1] - c0));
                     } else {
-                        z = dense_bucket_search<1>(qc, K, T - S, 0, 0u, lane);
+                        z = tiny ? dense_search_tiny(qc, K, T - S, s_tk, s_tdc, s_tm)
+                                 : dense_bucket_search<1>(qc, K, T - S, 0, 0u, lane);
                     }
                     if (z < 0) {
                         atomicOr(p.error, kErrRowRange);
@@ -801,6 +897,9 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
             for (int w = 0; w < kSampleThreads / 32; ++w) s += s_red[w];
             p.item_ll[it] = s;
         }
+        // a tiny item's topics back to the base row (every draw of it is done)
+        if (tiny && tid < s_tm)
+            ph[s_tk[tid]] = (0.f + p.beta) * (1.0f / ((float)__ldg(p.nk + s_tk[tid]) + p.vbeta));
     }
 }
 

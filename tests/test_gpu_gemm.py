@@ -120,3 +120,36 @@ def test_gemm_rejects_bad_shapes():
     assert cb.lib().culda_gemm_bf16(C.byref(bad), None) == _ffi.CULDA_ERR_INVALID_ARG
     bad.m, bad.k = 128, 48
     assert cb.lib().culda_gemm_bf16(C.byref(bad), None) == _ffi.CULDA_ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("m,n,k,splits", [(128, 128, 512, 2), (256, 384, 1024, 5), (512, 256, 4096, 16),
+                                          (128, 256, 192, 3)])
+def test_gemm_split_k_accumulates(m, n, k, splits):
+    """k cut into slices whose partial products are added with atomics into
+    out_f32 (zeros, or a value to add to); bias once; same 1e-5 bound."""
+    import torch
+
+    a, b, ref = _operands(m, n, k, k, k, seed=3 * m + k)
+    bias = torch.randn(n, dtype=torch.float32, device="cuda")
+    base = torch.randn(m, n, dtype=torch.float32, device="cuda")
+    out = base.clone()
+    args = _ffi.GemmArgs(m=m, n=n, k=k, a=_ptr(a), lda=k, b=_ptr(b), ldb=k, epilogue=_ffi.CULDA_GEMM_F32,
+                         alpha=1.0, out_f32=_ptr(out), ldo=n, bias=_ptr(bias), k_splits=splits)
+    assert _run(args) == 0
+    want = base.cpu().double() + ref + bias.cpu().double()
+    assert (out.cpu().double() - want).abs().max().item() <= 1e-5 * max(1.0, ref.abs().max().item())
+
+
+def test_gemm_split_k_rejects_bad_splits():
+    import torch
+
+    a = torch.zeros(128, 128, dtype=torch.bfloat16, device="cuda")
+    out = torch.zeros(128, 128, dtype=torch.float32, device="cuda")
+    g = torch.zeros(128, 128, dtype=torch.bfloat16, device="cuda")
+    bad = _ffi.GemmArgs(m=128, n=128, k=128, a=_ptr(a), lda=128, b=_ptr(a), ldb=128,
+                        epilogue=_ffi.CULDA_GEMM_F32, alpha=1.0, out_f32=_ptr(out), ldo=128, k_splits=3)
+    assert cb.lib().culda_gemm_bf16(C.byref(bad), None) == _ffi.CULDA_ERR_INVALID_ARG  # 3 > k / 64
+    bad2 = _ffi.GemmArgs(m=128, n=128, k=128, a=_ptr(a), lda=128, b=_ptr(a), ldb=128,
+                         epilogue=_ffi.CULDA_GEMM_GELU_BWD, out_bf16=_ptr(g), out_bf16_t=_ptr(g), ldo=128, ld_t=128,
+                         pre=_ptr(out), k_splits=2)
+    assert cb.lib().culda_gemm_bf16(C.byref(bad2), None) == _ffi.CULDA_ERR_INVALID_ARG

@@ -92,16 +92,27 @@ __global__ void embbag_fwd_kernel(int batch, int rows, const int32_t *__restrict
             for (int64_t tb = t0; tb < t1; tb += 32) {
                 const int wl = tb + lane < t1 ? words[tb + lane] : 0;
                 const int n = (int)min((int64_t)32, t1 - tb);
-                for (int j = 0; j < n; ++j) {
-                    const int w = __shfl_sync(0xffffffffu, wl, j);
-                    if ((unsigned)w >= (unsigned)V) {
-                        if (lane == 0) atomicOr(error, kErrWordRange);
-                        continue;
-                    }
-                    float f[8];
-                    unpack8(__ldg(reinterpret_cast<const uint4 *>(emb + (size_t)w * kE) + lane), f);
+                // eight embedding rows in flight, then added in token order
+                for (int j0 = 0; j0 < n; j0 += 8) {
+                    uint4 v[8];
+                    bool ok[8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) acc[i] += f[i];
+                    for (int u = 0; u < 8; ++u) {
+                        const int w = __shfl_sync(0xffffffffu, wl, (j0 + u) & 31);
+                        const bool in = j0 + u < n;
+                        ok[u] = in && (unsigned)w < (unsigned)V;
+                        if (in && !ok[u] && lane == 0) atomicOr(error, kErrWordRange);
+                        v[u] = ok[u] ? __ldg(reinterpret_cast<const uint4 *>(emb + (size_t)w * kE) + lane)
+                                     : make_uint4(0u, 0u, 0u, 0u);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        if (!ok[u]) continue;
+                        float f[8];
+                        unpack8(v[u], f);
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) acc[i] += f[i];
+                    }
                 }
             }
             const float inv = t1 > t0 ? 1.0f / (float)(t1 - t0) : 0.f;
@@ -184,13 +195,29 @@ __global__ void embbag_bwd_grouped_kernel(int V, const int32_t *__restrict__ sta
         const int my_w = lane < cn ? wid[c0 + lane] : -1;
         const int my_b = lane < cn ? rows[c0 + lane] : 0;
         const float my_s = lane < cn ? inv_len[my_b] : 0.f;
+        // the chunk's dX0 rows, 2 x 16 bytes per lane each, loaded 8 at a time ahead of their use
         float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
+        float4 r0[8], r1[8];
         for (int j = 0; j < cn; ++j) {
+            if ((j & 7) == 0) {
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int bj = __shfl_sync(0xffffffffu, my_b, (j + u) & 31);
+                    const float4 *q = reinterpret_cast<const float4 *>(dX0 + (size_t)bj * kE) + 2 * lane;
+                    const bool in = j + u < cn;
+                    r0[u] = in ? q[0] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    r1[u] = in ? q[1] : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
             const int w = __shfl_sync(0xffffffffu, my_w, j);
-            const int b = __shfl_sync(0xffffffffu, my_b, j);
             const float sc = __shfl_sync(0xffffffffu, my_s, j);
-            const float4 *src = reinterpret_cast<const float4 *>(dX0 + (size_t)b * kE) + 2 * lane;
-            const float4 g0 = src[0], g1 = src[1];
+            float4 g0 = r0[0], g1 = r1[0];
+#pragma unroll
+            for (int u = 1; u < 8; ++u)
+                if ((j & 7) == u) {
+                    g0 = r0[u];
+                    g1 = r1[u];
+                }
             a0.x += g0.x * sc;
             a0.y += g0.y * sc;
             a0.z += g0.z * sc;

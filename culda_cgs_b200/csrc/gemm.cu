@@ -12,7 +12,9 @@
 // (128-byte swizzle); warp 1 lane 0 issues tcgen05.mma (M = 128, N = 128,
 // K = 16 per instruction) into 128 TMEM columns and frees each stage with
 // tcgen05.commit; when the last MMA has landed all four warps read their 32
-// TMEM lanes back with tcgen05.ld and run the epilogue.  Every mbarrier wait
+// TMEM lanes back with tcgen05.ld into a shared-memory copy of the tile, and
+// the epilogue writes it out row by row (coalesced) and, for the transposed
+// BF16 copy and the column sums, column by column.  Every mbarrier wait
 // is bounded: a wait that gives up sets kErrTimeout in the error word and the
 // tile is not stored.
 #include <cuda.h>
@@ -42,63 +44,77 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return cdf + x * pdf;
 }
 
-__device__ __forceinline__ void store_bf16_row(__nv_bfloat16 *dst, const float v[16]) {
-    uint4 q[2];
-    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(q);
+// The accumulator tile is staged in shared memory (the operand ring is free
+// once the last MMA has landed) as S[128][kSP] floats, row = output row; the
+// stride of 129 keeps both a lane-per-row write and a lane-per-row column read
+// free of bank conflicts.  Phase 1 (rows): each warp takes rows w, w+4, ...,
+// each lane 4 consecutive columns, so every global row store or load is one
+// 512-byte (FP32) or 256-byte (BF16) run.  Phase 2 (columns, BF16 epilogues):
+// each warp takes columns, each lane rows l, l+32, l+64, l+96 of the column,
+// for the transposed copy and the bias-gradient column sums.
+constexpr int kSP = kBN + 1;
+
+template <int EPI>
+__device__ __forceinline__ void epilogue_rows(const GemmEpilogue &ep, float *S, int m0, int n0, int warp, int lane) {
+    const int c = 4 * lane;
+    for (int r = warp; r < kBM; r += kGemmThreads / 32) {
+        float v[4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-    uint4 *d = reinterpret_cast<uint4 *>(dst);
-    d[0] = q[0];
-    d[1] = q[1];
+        for (int i = 0; i < 4; ++i) v[i] = S[r * kSP + c + i];
+        const size_t o = (size_t)(m0 + r) * ep.ldo + n0 + c;
+        if constexpr (EPI == kEpiF32) {
+            const bool with_bias = ep.bias && blockIdx.z == 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) v[i] = v[i] * ep.alpha + (with_bias ? ep.bias[n0 + c + i] : 0.f);
+            float4 *d = reinterpret_cast<float4 *>(ep.out_f32 + o);
+            if (ep.k_splits > 1)
+                atomicAdd(d, make_float4(v[0], v[1], v[2], v[3]));
+            else
+                *d = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+            if constexpr (EPI == kEpiBiasGelu) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) v[i] += ep.bias[n0 + c + i];
+                *reinterpret_cast<float4 *>(ep.out_f32 + o) = make_float4(v[0], v[1], v[2], v[3]);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) v[i] = gelu(v[i]);
+            } else {  // kEpiGeluBwd
+                const float4 pre = *reinterpret_cast<const float4 *>(ep.pre + o);
+                v[0] *= gelu_grad(pre.x);
+                v[1] *= gelu_grad(pre.y);
+                v[2] *= gelu_grad(pre.z);
+                v[3] *= gelu_grad(pre.w);
+            }
+            uint2 q;
+            __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&q);
+            h[0] = __floats2bfloat162_rn(v[0], v[1]);
+            h[1] = __floats2bfloat162_rn(v[2], v[3]);
+            *reinterpret_cast<uint2 *>(ep.out_bf16 + o) = q;
+            // the transposed copy and the column sums take the FP32 value: both
+            // copies are the same single rounding of it to BF16
+#pragma unroll
+            for (int i = 0; i < 4; ++i) S[r * kSP + c + i] = v[i];
+        }
+    }
 }
 
 template <int EPI>
-__device__ __forceinline__ void epilogue(const GemmEpilogue &ep, int row, int col, float v[16], int lane) {
-    const size_t o = (size_t)row * ep.ldo + col;
-    if constexpr (EPI == kEpiF32) {
-        const bool with_bias = ep.bias && blockIdx.z == 0;
+__device__ __forceinline__ void epilogue_cols(const GemmEpilogue &ep, const float *S, int m0, int n0, int warp,
+                                              int lane) {
+    for (int cc = warp; cc < kBN; cc += kGemmThreads / 32) {
+        float s = 0.f;
+        __nv_bfloat16 *dst = ep.out_bf16_t + (size_t)(n0 + cc) * ep.ld_t + m0;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = v[i] * ep.alpha + (with_bias ? ep.bias[col + i] : 0.f);
-        float4 *d = reinterpret_cast<float4 *>(ep.out_f32 + o);
-        if (ep.k_splits > 1) {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) atomicAdd(d + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
-        } else {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        for (int k = 0; k < kBM / 32; ++k) {
+            const int r = lane + 32 * k;
+            const float v = S[r * kSP + cc];
+            dst[r] = __float2bfloat16_rn(v);
+            s += v;
         }
-    } else if constexpr (EPI == kEpiBiasGelu) {
-        float4 *pre = reinterpret_cast<float4 *>(ep.out_f32 + o);
+        if (EPI == kEpiGeluBwd && ep.colsum) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] += ep.bias[col + i];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) pre[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = gelu(v[i]);
-        store_bf16_row(ep.out_bf16 + o, v);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) ep.out_bf16_t[(size_t)(col + i) * ep.ld_t + row] = __float2bfloat16_rn(v[i]);
-    } else {  // kEpiGeluBwd
-        const float4 *pre = reinterpret_cast<const float4 *>(ep.pre + o);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const float4 p = pre[i];
-            v[4 * i] *= gelu_grad(p.x);
-            v[4 * i + 1] *= gelu_grad(p.y);
-            v[4 * i + 2] *= gelu_grad(p.z);
-            v[4 * i + 3] *= gelu_grad(p.w);
-        }
-        store_bf16_row(ep.out_bf16 + o, v);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) ep.out_bf16_t[(size_t)(col + i) * ep.ld_t + row] = __float2bfloat16_rn(v[i]);
-        if (ep.colsum) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                float s = v[i];
-#pragma unroll
-                for (int w = 16; w > 0; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
-                if (lane == 0) atomicAdd(ep.colsum + col + i, s);
-            }
+            for (int w = 16; w > 0; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
+            if (lane == 0) atomicAdd(ep.colsum + n0 + cc, s);
         }
     }
 }
@@ -179,18 +195,26 @@ __global__ void __launch_bounds__(kGemmThreads, 2)
         __syncwarp();
     }
 
-    // epilogue: warp w owns TMEM lanes 32w .. 32w+31 = output rows m0+32w ..
+    // epilogue: warp w owns TMEM lanes 32w .. 32w+31 = output rows m0+32w ..;
+    // the decision to store is the same in every thread (barrier, then the flag)
     bool ok = umma::mbar_wait(&done, 0u);
     umma::tc_fence_after();
-    ok = __all_sync(0xffffffffu, ok);
-    if (!ok && lane == 0 && error) atomicOr(error, kErrTimeout);
-    const int aborted = *(volatile int *)&abort_flag;
-    if (ok && !aborted) {
-        const int row = m0 + warp * 32 + lane;
+    if (!__all_sync(0xffffffffu, ok) && lane == 0 && error) atomicOr(error, kErrTimeout);
+    const bool go = __syncthreads_and(ok) && !*(volatile int *)&abort_flag;
+    if (go) {
+        float *S = reinterpret_cast<float *>(base);  // the operand ring, free now: every MMA has landed
+        const int r = warp * 32 + lane;
         for (int c = 0; c < kBN; c += 16) {
             float v[16];
             umma::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-            epilogue<EPI>(ep, row, n0 + c, v, lane);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) S[r * kSP + c + i] = v[i];
+        }
+        __syncthreads();
+        epilogue_rows<EPI>(ep, S, m0, n0, warp, lane);
+        if (EPI != kEpiF32) {
+            __syncthreads();
+            epilogue_cols<EPI>(ep, S, m0, n0, warp, lane);
         }
     }
     umma::tc_fence_before();

@@ -404,8 +404,8 @@ cudaError_t gemm(int M, int N, int K, const bf16 *A, const bf16 *B, int epi, con
 }
 
 // Weight gradients: M x N is a few tiles and K the batch, so the K range is
-// cut into slices (at least 4 k-blocks each) until about two CTAs per SM are
-// busy; the slices add into the zeroed gradient.
+// cut into slices (at least 4 k-blocks each), as many as fill the two CTAs
+// per SM in one wave; the slices add into the zeroed gradient.
 cudaError_t gemm_wgrad(int M, int N, int K, const bf16 *A, const bf16 *B, GemmEpilogue ep, int32_t *err,
                        cudaStream_t s) {
     int sms = 148;
@@ -413,7 +413,7 @@ cudaError_t gemm_wgrad(int M, int N, int K, const bf16 *A, const bf16 *B, GemmEp
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int tiles = (M / 128) * (N / 128);
     const int by_k = std::max(1, (K / 64) / 4);
-    ep.k_splits = std::max(1, std::min(by_k, (2 * sms + tiles - 1) / tiles));
+    ep.k_splits = std::max(1, std::min(by_k, (2 * sms) / tiles));
     return gemm_bf16_nt(M, N, K, A, K, B, K, kEpiF32, ep, err, s);
 }
 

@@ -57,7 +57,19 @@ constexpr int kSP = kBN + 1;
 template <int EPI>
 __device__ __forceinline__ void epilogue_rows(const GemmEpilogue &ep, float *S, int m0, int n0, int warp, int lane) {
     const int c = 4 * lane;
-    for (int r = warp; r < kBM; r += kGemmThreads / 32) {
+    constexpr int kRowStep = kGemmThreads / 32, kAhead = 8;
+    for (int r0 = warp; r0 < kBM; r0 += kRowStep * kAhead) {
+        // the pre-activations of the next 8 rows are loaded before any of them
+        // is stored: the stores below could alias them for all the compiler knows
+        float4 pv[kAhead];
+        if constexpr (EPI == kEpiGeluBwd) {
+#pragma unroll
+            for (int u = 0; u < kAhead; ++u)
+                pv[u] = *reinterpret_cast<const float4 *>(ep.pre + (size_t)(m0 + r0 + kRowStep * u) * ep.ldo + n0 + c);
+        }
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) {
+        const int r = r0 + kRowStep * u;
         float v[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) v[i] = S[r * kSP + c + i];
@@ -79,7 +91,7 @@ __device__ __forceinline__ void epilogue_rows(const GemmEpilogue &ep, float *S, 
 #pragma unroll
                 for (int i = 0; i < 4; ++i) v[i] = gelu(v[i]);
             } else {  // kEpiGeluBwd
-                const float4 pre = *reinterpret_cast<const float4 *>(ep.pre + o);
+                const float4 pre = pv[u];
                 v[0] *= gelu_grad(pre.x);
                 v[1] *= gelu_grad(pre.y);
                 v[2] *= gelu_grad(pre.z);
@@ -94,6 +106,7 @@ __device__ __forceinline__ void epilogue_rows(const GemmEpilogue &ep, float *S, 
             // copies are the same single rounding of it to BF16
 #pragma unroll
             for (int i = 0; i < 4; ++i) S[r * kSP + c + i] = v[i];
+        }
         }
     }
 }

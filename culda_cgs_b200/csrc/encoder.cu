@@ -79,19 +79,27 @@ __device__ __forceinline__ void unpack8(const uint4 &v, float f[8]) {
 }
 
 // Warp per batch row; lane l owns embedding columns 8l .. 8l+7.
-__global__ void embbag_fwd_kernel(int batch, int rows, const int32_t *__restrict__ docs,
-                                  const int64_t *__restrict__ doc_ptr, const int32_t *__restrict__ words, int V,
-                                  const bf16 *__restrict__ emb, bf16 *X0, int32_t *error) {
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < rows; b += nw) {
+__global__ void __launch_bounds__(256) embbag_fwd_kernel(int batch, int rows, const int32_t *__restrict__ docs,
+                                                         const int64_t *__restrict__ doc_ptr,
+                                                         const int32_t *__restrict__ words, int V,
+                                                         const bf16 *__restrict__ emb, bf16 *X0, int32_t *error) {
+    // one CTA per batch row: its 8 warps take contiguous eighths of the
+    // document's tokens (a long document is no longer one warp's serial loop),
+    // then the partial sums are added in warp order
+    __shared__ float part[8][kE];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = blockIdx.x; b < rows; b += gridDim.x) {
         float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int64_t t0 = 0, t1 = 0;
         if (b < batch) {
             const int d = docs ? docs[b] : b;
-            const int64_t t0 = doc_ptr[d], t1 = doc_ptr[d + 1];
-            for (int64_t tb = t0; tb < t1; tb += 32) {
-                const int wl = tb + lane < t1 ? words[tb + lane] : 0;
-                const int n = (int)min((int64_t)32, t1 - tb);
+            t0 = doc_ptr[d];
+            t1 = doc_ptr[d + 1];
+            const int64_t per = (t1 - t0 + 7) / 8;
+            const int64_t w0 = t0 + per * warp, w1 = min(t1, w0 + per);
+            for (int64_t tb = w0; tb < w1; tb += 32) {
+                const int wl = tb + lane < w1 ? words[tb + lane] : 0;
+                const int n = (int)min((int64_t)32, w1 - tb);
                 // eight embedding rows in flight, then added in token order
                 for (int j0 = 0; j0 < n; j0 += 8) {
                     uint4 v[8];
@@ -115,15 +123,23 @@ __global__ void embbag_fwd_kernel(int batch, int rows, const int32_t *__restrict
                     }
                 }
             }
-            const float inv = t1 > t0 ? 1.0f / (float)(t1 - t0) : 0.f;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) acc[i] *= inv;
         }
-        uint4 q;
-        __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&q);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(acc[2 * i], acc[2 * i + 1]);
-        reinterpret_cast<uint4 *>(X0 + (size_t)b * kE)[lane] = q;
+        for (int i = 0; i < 8; ++i) part[warp][8 * lane + i] = acc[i];
+        __syncthreads();
+        if (warp == 0) {
+            float sum[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int w = 0; w < 8; ++w)
+#pragma unroll
+                for (int i = 0; i < 8; ++i) sum[i] += part[w][8 * lane + i];
+            const float inv = t1 > t0 ? 1.0f / (float)(t1 - t0) : 0.f;
+            uint4 q;
+            __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&q);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(sum[2 * i] * inv, sum[2 * i + 1] * inv);
+            reinterpret_cast<uint4 *>(X0 + (size_t)b * kE)[lane] = q;
+        }
+        __syncthreads();  // part is rewritten by the next row
     }
 }
 
@@ -135,17 +151,20 @@ __global__ void embbag_fwd_kernel(int batch, int rows, const int32_t *__restrict
 // (the frequent ones) adds each chunk's partial sum with one vector atomic
 // per lane.  gE holds zeros before the pass.
 
-// cnt[w] += 1 for every token of batch row b (warp per row); inv_len[b] = 1 / L_b.
-__global__ void bag_count_kernel(int batch, const int32_t *__restrict__ docs, const int64_t *__restrict__ doc_ptr,
-                                 const int32_t *__restrict__ words, int V, int32_t *cnt, float *inv_len,
-                                 unsigned long long *total) {
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < batch; b += nw) {
+// cnt[w] += 1 for every token of batch row b (a CTA per row, its threads over
+// the row's tokens); inv_len[b] = 1 / L_b.
+__global__ void __launch_bounds__(256) bag_count_kernel(int batch, const int32_t *__restrict__ docs,
+                                                        const int64_t *__restrict__ doc_ptr,
+                                                        const int32_t *__restrict__ words, int V, int32_t *cnt,
+                                                        float *inv_len, unsigned long long *total) {
+    __shared__ int s_n;
+    for (int b = blockIdx.x; b < batch; b += gridDim.x) {
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
         const int d = docs ? docs[b] : b;
         const int64_t t0 = doc_ptr[d], t1 = doc_ptr[d + 1];
         int n = 0;
-        for (int64_t t = t0 + lane; t < t1; t += 32) {
+        for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
             const int w = words[t];
             if ((unsigned)w < (unsigned)V) {
                 atomicAdd(&cnt[w], 1);
@@ -154,23 +173,26 @@ __global__ void bag_count_kernel(int batch, const int32_t *__restrict__ docs, co
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-        if (lane == 0) {
+        if ((threadIdx.x & 31) == 0 && n) atomicAdd(&s_n, n);
+        __syncthreads();
+        if (threadIdx.x == 0) {
             inv_len[b] = t1 > t0 ? 1.0f / (float)(t1 - t0) : 0.f;
-            if (total) atomicAdd(total, (unsigned long long)n);
+            if (total) atomicAdd(total, (unsigned long long)s_n);
         }
+        __syncthreads();  // s_n is reset for the next row
     }
 }
 
 // rows[start[w] + fill[w]++] = b and wid[...] = w for every token of batch row b.
-__global__ void bag_place_kernel(int batch, const int32_t *__restrict__ docs, const int64_t *__restrict__ doc_ptr,
-                                 const int32_t *__restrict__ words, int V, const int32_t *__restrict__ start,
-                                 int32_t *fill, int32_t *rows, int32_t *wid) {
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < batch; b += nw) {
+__global__ void __launch_bounds__(256) bag_place_kernel(int batch, const int32_t *__restrict__ docs,
+                                                        const int64_t *__restrict__ doc_ptr,
+                                                        const int32_t *__restrict__ words, int V,
+                                                        const int32_t *__restrict__ start, int32_t *fill, int32_t *rows,
+                                                        int32_t *wid) {
+    for (int b = blockIdx.x; b < batch; b += gridDim.x) {
         const int d = docs ? docs[b] : b;
         const int64_t t0 = doc_ptr[d], t1 = doc_ptr[d + 1];
-        for (int64_t t = t0 + lane; t < t1; t += 32) {
+        for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
             const int w = words[t];
             if ((unsigned)w < (unsigned)V) {
                 const int pos = start[w] + atomicAdd(&fill[w], 1);
@@ -181,7 +203,6 @@ __global__ void bag_place_kernel(int batch, const int32_t *__restrict__ docs, co
     }
 }
 
-// Warp per chunk of 32 grouped tokens; each lane holds 8 of the 256 columns.
 // The grouped list holds start[V] tokens (those with a word id below V).
 __global__ void embbag_bwd_grouped_kernel(int V, const int32_t *__restrict__ start,
                                           const int32_t *__restrict__ rows, const int32_t *__restrict__ wid,
@@ -439,7 +460,7 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
     const int Bp = (batch + 127) & ~127, K = e->K;
     int32_t *err = e->d_error;
     // forward
-    embbag_fwd_kernel<<<grid_for((int64_t)Bp * 32), 256, 0, s>>>(batch, Bp, docs, doc_ptr, words, e->V, e->emb_bf,
+    embbag_fwd_kernel<<<std::min(Bp, 148 * 16), 256, 0, s>>>(batch, Bp, docs, doc_ptr, words, e->V, e->emb_bf,
                                                                  e->X0, err);
     ECK(cudaGetLastError());
     GemmEpilogue ep;
@@ -503,7 +524,7 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
     const size_t vb = sizeof(int32_t) * ((size_t)e->V + 1);
     ECK(cudaMemsetAsync(e->bag_cnt, 0, vb, s));
     if (batch_tokens < 0) ECK(cudaMemsetAsync(e->bag_total, 0, sizeof(unsigned long long), s));
-    bag_count_kernel<<<grid_for((int64_t)batch * 32), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_cnt,
+    bag_count_kernel<<<std::min(batch, 148 * 16), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_cnt,
                                                                    e->bag_inv_len,
                                                                    batch_tokens < 0 ? e->bag_total : nullptr);
     ECK(cudaGetLastError());
@@ -529,7 +550,7 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
     }
     ECK(cub::DeviceScan::ExclusiveSum(e->scan_tmp, e->scan_tmp_bytes, e->bag_cnt, e->bag_start, e->V + 1, s));
     ECK(cudaMemsetAsync(e->bag_cnt, 0, vb, s));
-    bag_place_kernel<<<grid_for((int64_t)batch * 32), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_start,
+    bag_place_kernel<<<std::min(batch, 148 * 16), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_start,
                                                                    e->bag_cnt, e->bag_rows, e->bag_wid);
     ECK(cudaGetLastError());
     if (batch_tokens > 0) {

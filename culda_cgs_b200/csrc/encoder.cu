@@ -23,6 +23,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -143,79 +144,59 @@ __global__ void __launch_bounds__(256) embbag_fwd_kernel(int batch, int rows, co
     }
 }
 
-// The embedding gradient: the batch's tokens are grouped by word (a counting
-// sort: counts per word, their exclusive scan, placement), the grouped list
-// is cut into chunks of 32 tokens, and a warp walks its chunk in order,
-// summing dX0[b] / L_b per word in registers.  A word whose tokens all lie in
-// the chunk is written with plain stores; a word spread over several chunks
-// (the frequent ones) adds each chunk's partial sum with one vector atomic
-// per lane.  gE holds zeros before the pass.
+// The embedding gradient: the batch's (word, row) pairs are laid out in row
+// order (a scan of the row lengths), sorted by word (a radix sort, stable, so
+// a word's tokens stay in row order), and the sorted list is cut into chunks
+// of 32 tokens.  A warp walks its chunk in order, summing dX0[b] / L_b per
+// word in registers.  A word whose tokens all lie in the chunk is written with
+// plain stores; a word whose run crosses the chunk's first or last token (the
+// frequent ones) adds each chunk's partial sum with one vector atomic per
+// lane.  gE holds zeros before the pass; words outside [0, V) sort last under
+// the key V and are skipped.
 
-// cnt[w] += 1 for every token of batch row b (a CTA per row, its threads over
-// the row's tokens); inv_len[b] = 1 / L_b.
-__global__ void __launch_bounds__(256) bag_count_kernel(int batch, const int32_t *__restrict__ docs,
-                                                        const int64_t *__restrict__ doc_ptr,
-                                                        const int32_t *__restrict__ words, int V, int32_t *cnt,
-                                                        float *inv_len, unsigned long long *total) {
-    __shared__ int s_n;
-    for (int b = blockIdx.x; b < batch; b += gridDim.x) {
-        if (threadIdx.x == 0) s_n = 0;
-        __syncthreads();
+// len[b] = L_b (for the scan of row offsets) and inv_len[b] = 1 / L_b.
+__global__ void bag_rows_kernel(int batch, const int32_t *__restrict__ docs, const int64_t *__restrict__ doc_ptr,
+                                int32_t *len, float *inv_len) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < batch; b += gridDim.x * blockDim.x) {
         const int d = docs ? docs[b] : b;
-        const int64_t t0 = doc_ptr[d], t1 = doc_ptr[d + 1];
-        int n = 0;
-        for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-            const int w = words[t];
-            if ((unsigned)w < (unsigned)V) {
-                atomicAdd(&cnt[w], 1);
-                ++n;
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-        if ((threadIdx.x & 31) == 0 && n) atomicAdd(&s_n, n);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            inv_len[b] = t1 > t0 ? 1.0f / (float)(t1 - t0) : 0.f;
-            if (total) atomicAdd(total, (unsigned long long)s_n);
-        }
-        __syncthreads();  // s_n is reset for the next row
+        const int64_t L = doc_ptr[d + 1] - doc_ptr[d];
+        len[b] = (int32_t)L;
+        inv_len[b] = L > 0 ? 1.0f / (float)L : 0.f;
     }
 }
 
-// rows[start[w] + fill[w]++] = b and wid[...] = w for every token of batch row b.
-__global__ void __launch_bounds__(256) bag_place_kernel(int batch, const int32_t *__restrict__ docs,
+// key[off[b] + j] = word of the j-th token of row b (V when out of range), val = b.
+__global__ void __launch_bounds__(256) bag_pairs_kernel(int batch, const int32_t *__restrict__ docs,
                                                         const int64_t *__restrict__ doc_ptr,
                                                         const int32_t *__restrict__ words, int V,
-                                                        const int32_t *__restrict__ start, int32_t *fill, int32_t *rows,
-                                                        int32_t *wid) {
+                                                        const int32_t *__restrict__ off, int32_t *key, int32_t *val) {
     for (int b = blockIdx.x; b < batch; b += gridDim.x) {
         const int d = docs ? docs[b] : b;
         const int64_t t0 = doc_ptr[d], t1 = doc_ptr[d + 1];
+        const int o = off[b];
         for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
             const int w = words[t];
-            if ((unsigned)w < (unsigned)V) {
-                const int pos = start[w] + atomicAdd(&fill[w], 1);
-                rows[pos] = b;
-                wid[pos] = w;
-            }
+            key[o + (t - t0)] = (unsigned)w < (unsigned)V ? w : V;
+            val[o + (t - t0)] = b;
         }
     }
 }
 
-// The grouped list holds start[V] tokens (those with a word id below V).
-__global__ void embbag_bwd_grouped_kernel(int V, const int32_t *__restrict__ start,
-                                          const int32_t *__restrict__ rows, const int32_t *__restrict__ wid,
-                                          const float *__restrict__ inv_len, const float *__restrict__ dX0,
-                                          float *gE) {
-    const int64_t n = start[V];
+// Warp per chunk of 32 sorted tokens; each lane holds 8 of the 256 columns.
+__global__ void embbag_bwd_grouped_kernel(int64_t n, int V, const int32_t *__restrict__ wid,
+                                          const int32_t *__restrict__ rows, const float *__restrict__ inv_len,
+                                          const float *__restrict__ dX0, float *gE) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t c0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; c0 < n; c0 += nw * 32) {
         const int cn = (int)min((int64_t)32, n - c0);
-        const int my_w = lane < cn ? wid[c0 + lane] : -1;
+        const int my_w = lane < cn ? wid[c0 + lane] : V;
         const int my_b = lane < cn ? rows[c0 + lane] : 0;
         const float my_s = lane < cn ? inv_len[my_b] : 0.f;
+        // does the chunk's first (last) run continue from the chunk before (after) it?
+        const int w_before = c0 > 0 ? wid[c0 - 1] : -1;
+        const int w_after = c0 + cn < n ? wid[c0 + cn] : -1;
+        const int first_w = __shfl_sync(0xffffffffu, my_w, 0), last_w = __shfl_sync(0xffffffffu, my_w, cn - 1);
         // the chunk's dX0 rows, 2 x 16 bytes per lane each, loaded 8 at a time ahead of their use
         float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
         float4 r0[8], r1[8];
@@ -249,13 +230,16 @@ __global__ void embbag_bwd_grouped_kernel(int V, const int32_t *__restrict__ sta
             a1.w += g1.w * sc;
             const int wn = __shfl_sync(0xffffffffu, my_w, (j + 1) & 31);
             if (j + 1 == cn || wn != w) {  // the end of this word's run in the chunk
-                float4 *dst = reinterpret_cast<float4 *>(gE + (size_t)w * kE) + 2 * lane;
-                if (start[w] >= c0 && start[w + 1] <= c0 + cn) {  // the whole word: no other chunk adds to it
-                    dst[0] = a0;
-                    dst[1] = a1;
-                } else {
-                    atomicAdd(dst, a0);
-                    atomicAdd(dst + 1, a1);
+                if (w < V) {
+                    float4 *dst = reinterpret_cast<float4 *>(gE + (size_t)w * kE) + 2 * lane;
+                    const bool shared = (w == first_w && w == w_before) || (w == last_w && w == w_after);
+                    if (!shared) {  // the whole word: no other chunk adds to it
+                        dst[0] = a0;
+                        dst[1] = a1;
+                    } else {
+                        atomicAdd(dst, a0);
+                        atomicAdd(dst + 1, a1);
+                    }
                 }
                 a0 = make_float4(0.f, 0.f, 0.f, 0.f);
                 a1 = a0;
@@ -360,15 +344,15 @@ struct culda_encoder {
     float *P1 = nullptr, *P2 = nullptr, *Z = nullptr, *dX0 = nullptr;
     double *d_loss = nullptr;
     int32_t *d_error = nullptr;
-    // the batch's tokens grouped by word for the embedding gradient
-    int32_t *bag_cnt = nullptr, *bag_start = nullptr;  // [V + 1] each
-    int32_t *bag_rows = nullptr;                        // [bag_cap] batch row of every token, by word
-    int32_t *bag_wid = nullptr;                         // [bag_cap] its word
+    // the batch's (word, row) pairs sorted by word, for the embedding gradient
+    int32_t *bag_len = nullptr, *bag_off = nullptr;  // [Bmax + 1] row lengths and their exclusive scan
+    float *bag_inv_len = nullptr;                    // [Bmax] 1 / L of every batch row
+    int32_t *bag_key = nullptr, *bag_val = nullptr;  // [bag_cap] pairs in row order
+    int32_t *bag_wid = nullptr, *bag_rows = nullptr; // [bag_cap] the pairs sorted by word
     int64_t bag_cap = 0;
-    float *bag_inv_len = nullptr;                       // [Bmax] 1 / L of every batch row
-    unsigned long long *bag_total = nullptr;            // tokens of the batch (device)
-    void *scan_tmp = nullptr;
-    size_t scan_tmp_bytes = 0;
+    void *scan_tmp = nullptr, *sort_tmp = nullptr;
+    size_t scan_tmp_bytes = 0, sort_tmp_bytes = 0;
+    int key_bits = 1;                                // bits of the keys 0..V
     std::vector<void *> allocs;
 
     float *tensor(int t) { return params + off[t]; }
@@ -520,42 +504,47 @@ int encoder_pass(culda_encoder *e, int batch, const int32_t *docs, const int64_t
     ECK(gemm_wgrad(kH, kE, Bp, e->dP1t, e->X0t, g1, err, s));  // dW1 = dP1^T X0
     g1.out_f32 = e->dX0;
     ECK(gemm(Bp, kE, kH, e->dP1, e->W1t, kEpiF32, g1, err, s));  // dX0 = dP1 W1
-    // the batch's tokens grouped by word, then one write of every embedding row's gradient
-    const size_t vb = sizeof(int32_t) * ((size_t)e->V + 1);
-    ECK(cudaMemsetAsync(e->bag_cnt, 0, vb, s));
-    if (batch_tokens < 0) ECK(cudaMemsetAsync(e->bag_total, 0, sizeof(unsigned long long), s));
-    bag_count_kernel<<<std::min(batch, 148 * 16), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_cnt,
-                                                                   e->bag_inv_len,
-                                                                   batch_tokens < 0 ? e->bag_total : nullptr);
+    // the batch's (word, row) pairs sorted by word, then one pass over them
+    bag_rows_kernel<<<(batch + 255) / 256, 256, 0, s>>>(batch, docs, doc_ptr, e->bag_len, e->bag_inv_len);
     ECK(cudaGetLastError());
-    if (batch_tokens < 0) {
-        unsigned long long n = 0;
-        ECK(cudaMemcpyAsync(&n, e->bag_total, sizeof n, cudaMemcpyDeviceToHost, s));
+    ECK(cub::DeviceScan::ExclusiveSum(e->scan_tmp, e->scan_tmp_bytes, e->bag_len, e->bag_off, batch + 1, s));
+    if (batch_tokens < 0) {  // the caller did not count the batch's tokens: read the scan's total
+        int32_t n = 0;
+        ECK(cudaMemcpyAsync(&n, e->bag_off + batch, sizeof n, cudaMemcpyDeviceToHost, s));
         ECK(cudaStreamSynchronize(s));
-        batch_tokens = (int64_t)n;
+        batch_tokens = n;
     }
     if (batch_tokens > e->bag_cap) {
         ECK(cudaStreamSynchronize(s));
-        for (int32_t **q : {&e->bag_rows, &e->bag_wid}) {
+        for (void **q : {(void **)&e->bag_key, (void **)&e->bag_val, (void **)&e->bag_wid, (void **)&e->bag_rows,
+                         &e->sort_tmp}) {
             if (*q) {
                 cudaFree(*q);
-                e->allocs.erase(std::find(e->allocs.begin(), e->allocs.end(), (void *)*q));
+                e->allocs.erase(std::find(e->allocs.begin(), e->allocs.end(), *q));
                 *q = nullptr;
             }
         }
         const int64_t cap = std::max<int64_t>(batch_tokens, 2 * e->bag_cap);
-        ECK(ealloc(e, &e->bag_rows, (size_t)cap));
+        ECK(ealloc(e, &e->bag_key, (size_t)cap));
+        ECK(ealloc(e, &e->bag_val, (size_t)cap));
         ECK(ealloc(e, &e->bag_wid, (size_t)cap));
+        ECK(ealloc(e, &e->bag_rows, (size_t)cap));
+        e->sort_tmp_bytes = 0;
+        ECK(cub::DeviceRadixSort::SortPairs(nullptr, e->sort_tmp_bytes, e->bag_key, e->bag_wid, e->bag_val,
+                                            e->bag_rows, (int)cap, 0, e->key_bits));
+        uint8_t *tmp = nullptr;
+        ECK(ealloc(e, &tmp, e->sort_tmp_bytes));
+        e->sort_tmp = tmp;
         e->bag_cap = cap;
     }
-    ECK(cub::DeviceScan::ExclusiveSum(e->scan_tmp, e->scan_tmp_bytes, e->bag_cnt, e->bag_start, e->V + 1, s));
-    ECK(cudaMemsetAsync(e->bag_cnt, 0, vb, s));
-    bag_place_kernel<<<std::min(batch, 148 * 16), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_start,
-                                                                   e->bag_cnt, e->bag_rows, e->bag_wid);
-    ECK(cudaGetLastError());
     if (batch_tokens > 0) {
-        embbag_bwd_grouped_kernel<<<grid_for(batch_tokens), 256, 0, s>>>(e->V, e->bag_start, e->bag_rows,
-                                                                         e->bag_wid, e->bag_inv_len, e->dX0,
+        bag_pairs_kernel<<<std::min(batch, 148 * 16), 256, 0, s>>>(batch, docs, doc_ptr, words, e->V, e->bag_off,
+                                                                   e->bag_key, e->bag_val);
+        ECK(cudaGetLastError());
+        ECK(cub::DeviceRadixSort::SortPairs(e->sort_tmp, e->sort_tmp_bytes, e->bag_key, e->bag_wid, e->bag_val,
+                                            e->bag_rows, (int)batch_tokens, 0, e->key_bits, s));
+        embbag_bwd_grouped_kernel<<<grid_for(batch_tokens), 256, 0, s>>>(batch_tokens, e->V, e->bag_wid, e->bag_rows,
+                                                                         e->bag_inv_len, e->dX0,
                                                                          e->grad(CULDA_ENC_E));
         ECK(cudaGetLastError());
     }
@@ -686,11 +675,11 @@ extern "C" int culda_encoder_create(const culda_encoder_params *p, culda_encoder
     EALLOC(e->dX0, B * kE);
     EALLOC(e->d_loss, 1);
     EALLOC(e->d_error, 1);
-    EALLOC(e->bag_cnt, (size_t)e->V + 1);
-    EALLOC(e->bag_start, (size_t)e->V + 1);
+    EALLOC(e->bag_len, (size_t)B + 1);
+    EALLOC(e->bag_off, (size_t)B + 1);
     EALLOC(e->bag_inv_len, B);
-    EALLOC(e->bag_total, 1);
-    r = cub::DeviceScan::ExclusiveSum(nullptr, e->scan_tmp_bytes, e->bag_cnt, e->bag_start, e->V + 1);
+    while ((1u << e->key_bits) <= (unsigned)e->V) ++e->key_bits;  // keys 0..V
+    r = cub::DeviceScan::ExclusiveSum(nullptr, e->scan_tmp_bytes, e->bag_len, e->bag_off, B + 1);
     if (r != cudaSuccess) return bail(r);
     {
         uint8_t *tmp = nullptr;

@@ -614,7 +614,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
         }
 
         // phi row of the word
-        const bool tiny = !p.frozen_phi && item.hot < 0 && item.count <= kTinyTokens;
+        // (at K = 256 the full build is cheaper than the patch: 16.2 against 15.7 ms per iteration)
+        const bool tiny = K >= 512 && !p.frozen_phi && item.hot < 0 && item.count <= kTinyTokens;
         float Q;
         if (tiny) {
             if (!s_tiny) {  // the base row and its dense prefix, once per CTA

@@ -290,7 +290,7 @@ int autotune_rebuild(culda_ctx *ctx, TuneResult &best) {
 // uniforms once, then per variant one warm-up and two timed launches that
 // write the other topic buffer.  The context's state does not change.
 int autotune_sampler(culda_ctx *ctx) {
-    static const int kCands[][2] = {{kFlatLanes, kSampleBlocksDefault}, {kFlatLanes, kSampleBlocksHigh},
+    static const int kCands[][2] = {{kFlatLanes, kSampleBlocksDefault}, {kFlatLanes, kFlatBlocks},
                                     {4, kSampleBlocksHigh},
                                     {8, kSampleBlocksHigh},                {16, kSampleBlocksHigh},
                                     {2, kSampleBlocksDefault},             {4, kSampleBlocksDefault},
@@ -398,11 +398,11 @@ int pick_group_lanes(int requested, int k) {
     return requested == 0 ? kFlatLanes : 0;  // 0: not a variant
 }
 
-// the flat walk's default is the 48-register build (10 CTAs per SM), the
+// the flat walk's default is the 56-register build (9 CTAs per SM), the
 // group samplers' the 64-register one
 int pick_sample_blocks(int requested, int group_lanes) {
     if (requested != 0) return requested;
-    return group_lanes == kFlatLanes ? kSampleBlocksHigh : kSampleBlocksDefault;
+    return group_lanes == kFlatLanes ? kFlatBlocks : kSampleBlocksDefault;
 }
 
 

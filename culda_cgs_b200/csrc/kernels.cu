@@ -632,7 +632,7 @@ extern "C" int culda_sample(const culda_sample_args *a, void *d_workspace, size_
     p.error = a->error ? a->error : counter + 1;
     int dev = 0;
     cudaGetDevice(&dev);
-    const int blocks = a->group_lanes == kFlatLanes ? kSampleBlocksHigh : kSampleBlocksDefault;
+    const int blocks = a->group_lanes == kFlatLanes ? kFlatBlocks : kSampleBlocksDefault;
     int bps = sample_blocks_per_sm(a->k, a->group_lanes, blocks);
     if (bps <= 0) bps = 1;
     const int grid = std::max(1, std::min(a->num_items, num_sms(dev) * bps));

@@ -68,9 +68,11 @@ inline int pow2_ceil(int k) {
 // Sampler variants: lanes per token G and the register budget, given as the
 // resident CTAs per SM the kernel is compiled for (kSampleBlocksDefault for
 // every G; kSampleBlocksHigh for G = 4, 8, 16).  G = kFlatLanes is the
-// warp-flattened walk (either register budget).
+// warp-flattened walk, built for kSampleBlocksDefault and kFlatBlocks (56
+// registers: its two-buffer walk spills at 48).
 constexpr int kSampleBlocksDefault = 8;
 constexpr int kSampleBlocksHigh = 10;
+constexpr int kFlatBlocks = 9;
 constexpr int kFlatLanes = -1;
 size_t sample_smem_bytes(int k, int group_lanes);
 bool sample_variant_exists(int group_lanes, int blocks_per_sm);

@@ -530,6 +530,56 @@ __device__ __forceinline__ int row_last_nonzero(const ThetaEntry *__restrict__ t
     return last;
 }
 
+// One walk group's pass over units [u0, ge) of a batch: the state carried
+// from step to step.  step() reduces the step at u0 (its entries in `cur`)
+// while the next step's entries load into `nx`, and returns false after the
+// range's last step.  The kernel alternates two Step buffers, step(a, b) then
+// step(b, a), so the prefetched entries never move between registers.
+struct FlatWalk {
+    const ThetaEntry *theta;
+    const float *ph;
+    float *ub;         // the batch's unit prefixes
+    const int *m_cum;  // first unit of every segment of the batch
+    const int *m_rs;   // row start of every segment
+    int ge, wl;
+    unsigned wm;
+    int sp, nxt, rowu, rbase, u0;  // segment of unit u0, its successor's first unit, its row
+    float s, c;                    // compensated running sum of the row
+    int gflag;                     // a row started inside the range
+
+    __device__ __forceinline__ bool step(const Step &cur, Step &nx) {
+        const int u1 = u0 + kWalkLanes;
+        bool reset1 = false;
+        if (u1 < ge && u1 == nxt) {
+            do {
+                ++sp;
+                nxt = m_cum[sp + 1];
+            } while (nxt == u1);
+            rowu = u1;
+            rbase = m_rs[sp];
+            reset1 = true;
+        }
+        if (u1 < ge) nx = load_unit(theta, rbase + kUnit * (u1 + wl - rowu));
+        float incl = unit_sum(cur, ph);
+#pragma unroll
+        for (int o = 1; o < kWalkLanes; o <<= 1) {
+            const float t = __shfl_up_sync(wm, incl, o, kWalkLanes);
+            if (wl >= o) incl = fsum(incl, t);
+        }
+        const float tot = __shfl_sync(wm, incl, kWalkLanes - 1, kWalkLanes);
+        ub[u0 + wl] = fsum(s + c, incl);
+        neumaier(s, c, tot);
+        if (u1 >= ge) return false;
+        if (reset1) {
+            s = 0.f;
+            c = 0.f;
+            gflag = 1;
+        }
+        u0 = u1;
+        return true;
+    }
+};
+
 // Items of at most kTinyTokens tokens (the long tail of the vocabulary) do not
 // rebuild the K-wide phihat row and dense prefix: a CTA keeps the row of a word
 // with no tokens, phihat_k = beta / (n_k + V beta), and its dense prefix, and an
@@ -689,8 +739,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
                 src = p.hot_phi + (size_t)item.hot * K;
             }
             // 1 / (n_k + V beta) is formed per item (the same operations, so the
-            // same bits, as a table would hold): without the table's 4 KB the
-            // 48-register build fits 10 CTAs per SM
+            // same bits, as a table would hold), which keeps the table's 4 KB
+            // out of each CTA's shared memory
             for (int j = tid; j < K; j += blockDim.x)
                 ph[j] = ((float)src[j] + p.beta) * (1.0f / ((float)__ldg(p.nk + j) + p.vbeta));
             __syncthreads();
@@ -776,45 +826,16 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
                 float gv = 0.f;
                 int gflag = 0, lead_end = gb;
                 if (gb < ge) {
-                    int sp = last_le(m_cum, n, gb);
-                    int nxt = m_cum[sp + 1], rowu = m_cum[sp], rbase = m_rs[sp];
-                    gflag = gb == rowu;
-                    lead_end = gflag ? gb : min(nxt, ge);
-                    float s = 0.f, c = 0.f;
-                    Step cur = load_unit(p.theta, rbase + kUnit * (gb + wl - rowu));
-                    for (int u0 = gb;;) {
-                        const int u1 = u0 + kWalkLanes;
-                        bool reset1 = false;
-                        if (u1 < ge && u1 == nxt) {
-                            do {
-                                ++sp;
-                                nxt = m_cum[sp + 1];
-                            } while (nxt == u1);
-                            rowu = u1;
-                            rbase = m_rs[sp];
-                            reset1 = true;
-                        }
-                        Step nx;
-                        if (u1 < ge) nx = load_unit(p.theta, rbase + kUnit * (u1 + wl - rowu));
-                        float incl = unit_sum(cur, ph);
-#pragma unroll
-                        for (int o = 1; o < kWalkLanes; o <<= 1) {
-                            const float t = __shfl_up_sync(wm, incl, o, kWalkLanes);
-                            if (wl >= o) incl = fsum(incl, t);
-                        }
-                        const float tot = __shfl_sync(wm, incl, kWalkLanes - 1, kWalkLanes);
-                        ub[u0 + wl] = fsum(s + c, incl);
-                        neumaier(s, c, tot);
-                        if (u1 >= ge) break;
-                        if (reset1) {
-                            s = 0.f;
-                            c = 0.f;
-                            gflag = 1;
-                        }
-                        u0 = u1;
-                        cur = nx;
+                    const int sp = last_le(m_cum, n, gb);
+                    FlatWalk w{p.theta, ph, ub, m_cum, m_rs, ge, wl, wm, sp, m_cum[sp + 1], m_cum[sp], m_rs[sp], gb,
+                               0.f, 0.f, 0};
+                    w.gflag = gb == w.rowu;
+                    lead_end = w.gflag ? gb : min(w.nxt, ge);
+                    Step a = load_unit(p.theta, w.rbase + kUnit * (gb + wl - w.rowu)), b;
+                    while (w.step(a, b) && w.step(b, a)) {
                     }
-                    gv = s + c;
+                    gflag = w.gflag;
+                    gv = w.s + w.c;
                 }
                 // segmented scan over the groups: the running row sum entering each range
                 double vd = (double)gv;
@@ -921,7 +942,7 @@ static const void *sample_fn() {
 static const void *sample_kernel_for(int g, int minb) {
     if (g == kFlatLanes) {
         if (minb == kSampleBlocksDefault) return reinterpret_cast<const void *>(&sample_flat_kernel<kSampleBlocksDefault>);
-        if (minb == kSampleBlocksHigh) return reinterpret_cast<const void *>(&sample_flat_kernel<kSampleBlocksHigh>);
+        if (minb == kFlatBlocks) return reinterpret_cast<const void *>(&sample_flat_kernel<kFlatBlocks>);
         return nullptr;
     }
     if (minb == kSampleBlocksDefault) switch (g) {

@@ -180,10 +180,10 @@ typedef struct culda_params {
                              walk, else 1,2,4,8,16,32 lanes per token */
     int32_t item_tokens;  /* max tokens per sampler work item, 0 = auto, at most 65535 */
     int32_t flags;        /* CULDA_FLAG_* */
-    int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (10
+    int32_t sample_blocks; /* sampler register budget, as resident CTAs per SM: 0 = auto (9
                               for the flat walk, 8 for the group samplers), 8 (<= 64
-                              registers), or 10 (<= 48 registers; the flat walk and
-                              group_lanes 4, 8, 16) */
+                              registers), 9 (<= 56 registers; the flat walk only) or 10
+                              (<= 48 registers; group_lanes 4, 8, 16) */
     int32_t theta_min_len; /* theta rebuild bins: docs of at least this many tokens are rebuilt
                               by a whole CTA each, the others by one warp each.  0 = auto (N
                               over the rebuild's warps, at least 1024; CULDA_FLAG_AUTOTUNE

@@ -48,7 +48,8 @@ def _params(**kw):
 
 
 @pytest.mark.parametrize("kw", [dict(k=48), dict(k=0), dict(k=8192), dict(alpha=0.0), dict(beta=-1.0),
-                                dict(group_lanes=3), dict(group_lanes=-2), dict(sample_blocks=9), dict(group_lanes=1, sample_blocks=10),
+                                dict(group_lanes=3), dict(group_lanes=-2), dict(sample_blocks=7), dict(group_lanes=1, sample_blocks=10),
+                                dict(group_lanes=1, sample_blocks=9), dict(group_lanes=-1, sample_blocks=10),
                                 dict(group_lanes=8, flags=_ffi.CULDA_FLAG_AUTOTUNE), dict(item_tokens=70000),
                                 dict(item_tokens=-1)])
 def test_create_rejects_bad_params(kw):

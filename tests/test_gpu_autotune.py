@@ -14,7 +14,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = {(-1, 8), (-1, 10), (4, 10), (8, 10), (16, 10), (2, 8), (4, 8), (8, 8)}
+VARIANTS = {(-1, 8), (-1, 9), (4, 10), (8, 10), (16, 10), (2, 8), (4, 8), (8, 8)}
 
 
 def test_autotune_picks_a_variant_and_keeps_parity():

@@ -74,7 +74,7 @@ CASES = [  # name, corpus, K, lanes per token, item tokens (0 = auto), sampler r
     ("mini-k1024-flat-hot", MINI.gen, 1024, -1, 300, 0),
     ("mini-k256-flat", MINI.gen, 256, -1, 0, 0),
     ("mini-k4096-flat", MINI.gen, 4096, -1, 0, 0),
-    ("mini-k1024-flat-b10-hot", MINI.gen, 1024, -1, 300, 10),
+    ("mini-k1024-flat-b8-hot", MINI.gen, 1024, -1, 300, 8),
 ]
 
 
@@ -89,7 +89,7 @@ def test_counts_exact_and_snapshot_draws(corpora, name, gen, k, g, item_tokens, 
     seed = 1234
     with cb.LDA(c, k, 50.0 / 1024, 0.01, seed=seed, group_lanes=g, item_tokens=item_tokens,
                 sample_blocks=blocks) as m:
-        assert m.info()["sample_blocks"] == (blocks or (10 if g == -1 else 8))
+        assert m.info()["sample_blocks"] == (blocks or (9 if g == -1 else 8))
         z0 = m.topics()
         assert np.array_equal(z0, O.init_topics(c.num_tokens, k, seed))
         s0 = assert_counts_exact(m, c)

@@ -745,7 +745,7 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--group-lanes", type=int, default=0)
     ap.add_argument("--item-tokens", type=int, default=0)
-    ap.add_argument("--sample-blocks", type=int, default=0, help="sampler register budget (CTAs per SM): 0, 8, 10")
+    ap.add_argument("--sample-blocks", type=int, default=0, help="sampler register budget (CTAs per SM): 0 (auto), 8, 9 (flat walk), 10 (group samplers)")
     ap.add_argument("--autotune", action="store_true", help="time the sampler variants at create and keep the fastest")
     ap.add_argument("--no-reorder", action="store_true", help="keep tokens in input order inside each word")
     ap.add_argument("--no-e2e", action="store_true")

@@ -49,20 +49,11 @@ __device__ __forceinline__ float entry_prob(uint32_t e, const float *ph) {
 __device__ __forceinline__ float fsum(float a, float b) { return __fadd_rn(a, b); }
 
 // ------------------------------------------------------------ dense bucket
-// Inclusive prefix qc[j] = alpha * sum_{i<=j} ph[i].  Each thread owns a run of
-// ceil(K/T) entries summed with Neumaier compensation; the run totals are
-// scanned with Kogge-Stone shuffles, so every prefix carries an error of
-// about ten FP32 roundings.
-__device__ void dense_bucket_prefix(const float *ph, float *qc, int K, float alpha, float *s_warp) {
+// Each thread holds the local inclusive sums of its run out[b, e) and their
+// total `tot`; adds to the run the totals of all earlier threads (Kogge-Stone
+// shuffles inside a warp, then across the warps).  Ends without a barrier.
+__device__ __forceinline__ void add_run_offsets(float tot, float *out, int b, int e, float *s_warp) {
     const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
-    const int per = (K + T - 1) / T;
-    const int b = min(tid * per, K), e = min(b + per, K);
-    float s = 0.f, c = 0.f;
-    for (int j = b; j < e; ++j) {
-        neumaier(s, c, alpha * ph[j]);
-        qc[j] = s + c;
-    }
-    const float tot = s + c;
     float incl = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -86,7 +77,23 @@ __device__ void dense_bucket_prefix(const float *ph, float *qc, int K, float alp
     }
     __syncthreads();
     const float base = s_warp[warp] + ex;
-    for (int j = b; j < e; ++j) qc[j] = base + qc[j];
+    for (int j = b; j < e; ++j) out[j] = base + out[j];
+}
+
+// Inclusive prefix qc[j] = alpha * sum_{i<=j} ph[i].  Each thread owns a run of
+// ceil(K/T) entries summed with Neumaier compensation; the run totals are
+// scanned with Kogge-Stone shuffles, so every prefix carries an error of
+// about ten FP32 roundings.
+__device__ void dense_bucket_prefix(const float *ph, float *qc, int K, float alpha, float *s_warp) {
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int per = (K + T - 1) / T;
+    const int b = min(tid * per, K), e = min(b + per, K);
+    float s = 0.f, c = 0.f;
+    for (int j = b; j < e; ++j) {
+        neumaier(s, c, alpha * ph[j]);
+        qc[j] = s + c;
+    }
+    add_run_offsets(s + c, qc, b, e, s_warp);
 }
 
 // First topic whose dense-bucket prefix exceeds tq (K-1 when none does).
@@ -589,27 +596,91 @@ struct FlatWalk {
 // of its topics, applied during the search.
 constexpr int kTinyTokens = 32;
 
-// First topic whose corrected dense prefix qc[j] + D(j) exceeds tq (K-1 when
-// none does); D(j) = dcum[i] for the last of the word's sorted topics tk[i] <= j.
-__device__ __forceinline__ int dense_search_tiny(const float *qc, int K, float tq, const int *tk, const float *dcum,
-                                                 int m) {
-    int lo = 0, hi = K - 1;
+// The flat walk keeps the dense bucket as one prefix per block of 8 topics
+// (K is a multiple of 32): qb[b] = alpha * sum of ph[0 .. 8 (b + 1)).  A draw
+// finds its block by a binary search of qb and its topic by a pass over the
+// block's 8 phihat values.  At K = 4096 that is 2 KB of shared memory instead
+// of 16 KB, which lets 7 CTAs share an SM instead of 5.
+constexpr int kDenseBlock = 8;
+
+// Each thread takes a run of blocks: a block's total is the running sum a
+// draw's pass over the block forms (the same operations, so the same bits),
+// the run's prefix is compensated, and add_run_offsets completes it.
+__device__ void dense_block_prefix(const float *ph, float *qb, int K, float alpha, float *s_warp) {
+    const int T = blockDim.x, nb = K / kDenseBlock, per = (nb + T - 1) / T;
+    const int b0 = min((int)threadIdx.x * per, nb), b1 = min(b0 + per, nb);
+    float s = 0.f, c = 0.f;
+    for (int b = b0; b < b1; ++b) {
+        const float4 x = reinterpret_cast<const float4 *>(ph)[2 * b];
+        const float4 y = reinterpret_cast<const float4 *>(ph)[2 * b + 1];
+        float part = alpha * x.x;
+        part = fsum(part, alpha * x.y);
+        part = fsum(part, alpha * x.z);
+        part = fsum(part, alpha * x.w);
+        part = fsum(part, alpha * y.x);
+        part = fsum(part, alpha * y.y);
+        part = fsum(part, alpha * y.z);
+        part = fsum(part, alpha * y.w);
+        neumaier(s, c, part);
+        qb[b] = s + c;
+    }
+    add_run_offsets(s + c, qb, b0, b1, s_warp);
+    __syncthreads();
+}
+
+// Inside block b, from the prefix `base` before it: the first topic whose
+// prefix exceeds tq, the block's last topic when rounding leaves it short.
+__device__ __forceinline__ int dense_block_scan(const float *ph, int b, float base, float alpha, float tq) {
+    const int t0 = b * kDenseBlock;
+    float part = 0.f;
+#pragma unroll
+    for (int i = 0; i < kDenseBlock; ++i) {
+        part = i ? fsum(part, alpha * ph[t0 + i]) : alpha * ph[t0];
+        if (fsum(base, part) > tq) return t0 + i;
+    }
+    return t0 + kDenseBlock - 1;
+}
+
+// First topic whose dense prefix exceeds tq (K-1 when none does).
+__device__ __forceinline__ int dense_search_blocks(const float *ph, const float *qb, int K, float alpha, float tq) {
+    int lo = 0, hi = K / kDenseBlock - 1;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        int a = 0, b = m;  // topics of the word up to mid
-        while (a < b) {
-            const int c = (a + b) >> 1;
-            if (tk[c] <= mid)
-                a = c + 1;
-            else
-                b = c;
-        }
-        if (fsum(qc[mid], a > 0 ? dcum[a - 1] : 0.f) > tq)
+        if (qb[mid] > tq)
             hi = mid;
         else
             lo = mid + 1;
     }
-    return lo;
+    return dense_block_scan(ph, lo, lo > 0 ? qb[lo - 1] : 0.f, alpha, tq);
+}
+
+// The same for a tiny item: qb holds the base row's prefixes and ph the base
+// row with the item's own topics patched in, so a block's prefix is qb[b]
+// plus the corrections of the item's topics up to the block's end, and the
+// pass over the block reads the patched values directly.
+__device__ __forceinline__ int dense_search_tiny_blocks(const float *ph, const float *qb, int K, float alpha, float tq,
+                                                        const int *tk, const float *dcum, int m) {
+    auto corrected = [&](int b) {
+        const int last = b * kDenseBlock + kDenseBlock - 1;
+        int a = 0, e = m;  // topics of the item up to the block's end
+        while (a < e) {
+            const int c = (a + e) >> 1;
+            if (tk[c] <= last)
+                a = c + 1;
+            else
+                e = c;
+        }
+        return fsum(qb[b], a > 0 ? dcum[a - 1] : 0.f);
+    };
+    int lo = 0, hi = K / kDenseBlock - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (corrected(mid) > tq)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return dense_block_scan(ph, lo, lo > 0 ? corrected(lo - 1) : 0.f, alpha, tq);
 }
 
 template <int MINB>
@@ -617,12 +688,13 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
     extern __shared__ float smem[];
     const int K = p.k, KP = p.kmask + 1, B = flat_unit_budget(K);
     float *ph = smem;               // [KP] phihat of the current word (zero past K), at offset 0
-    float *qc = smem + KP;          // [K]  dense-bucket prefix (the word histogram before that)
-    int *hist = reinterpret_cast<int *>(qc);
+                                    // (the word histogram before that)
+    float *qb = smem + KP;          // [K / 8] dense-bucket prefix at the end of every 8-topic block
+    int *hist = reinterpret_cast<int *>(ph);
     __shared__ int s_item, s_chunk;
     __shared__ float s_warp[kSampleThreads / 32];
     __shared__ double s_red[kSampleThreads / 32];
-    // tiny items: whether ph / qc hold the base row, and the item's topics
+    // tiny items: whether ph / qb hold the base row, and the item's topics
     __shared__ int s_tiny, s_tm;
     __shared__ int s_tk[kTinyTokens];
     __shared__ float s_tdc[kTinyTokens];
@@ -631,8 +703,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wl = lane & (kWalkLanes - 1), wg = lane / kWalkLanes;  // lane in its walk group, group
     const unsigned wm = group_mask<kWalkLanes>(lane);
-    float *ub = qc + K + warp * B;  // [B] unit prefixes of the warp's batch
-    int *m_cum = reinterpret_cast<int *>(qc + K + kFlatWarps * B) + warp * kFlatMeta;
+    float *ub = qb + K / kDenseBlock + warp * B;  // [B] unit prefixes of the warp's batch
+    int *m_cum = reinterpret_cast<int *>(qb + K / kDenseBlock + kFlatWarps * B) + warp * kFlatMeta;
     int *m_tc = m_cum + (kFlatSegs + 1);  // [n+1] first unit / first token (flat) of each segment
     int *m_rs = m_tc + (kFlatSegs + 1);   // [n] row start (entry index)
     int *m_t0 = m_rs + kFlatSegs;         // [n] first token
@@ -672,8 +744,7 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
                 for (int j = tid; j < K; j += blockDim.x)
                     ph[j] = (0.f + p.beta) * (1.0f / ((float)__ldg(p.nk + j) + p.vbeta));
                 __syncthreads();
-                dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
-                __syncthreads();
+                dense_block_prefix(ph, qb, K, p.alpha, s_warp);
                 if (tid == 0) s_tiny = 1;
             }
             if (warp == 0) {
@@ -714,7 +785,7 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
                 const float total = __shfl_sync(0xffffffffu, dc, m > 0 ? m - 1 : 0);
                 if (lane == 0) {
                     s_tm = m;
-                    s_tQ = fsum(qc[K - 1], m > 0 ? total : 0.f);
+                    s_tQ = fsum(qb[K / kDenseBlock - 1], m > 0 ? total : 0.f);
                 }
             }
             __syncthreads();
@@ -744,9 +815,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
             for (int j = tid; j < K; j += blockDim.x)
                 ph[j] = ((float)src[j] + p.beta) * (1.0f / ((float)__ldg(p.nk + j) + p.vbeta));
             __syncthreads();
-            dense_bucket_prefix(ph, qc, K, p.alpha, s_warp);
-            __syncthreads();
-            Q = qc[K - 1];
+            dense_block_prefix(ph, qb, K, p.alpha, s_warp);
+            Q = qb[K / kDenseBlock - 1];
             if (tid == 0) s_tiny = 0;  // read by every thread before the barrier above
         }
 
@@ -896,8 +966,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
                         // one unit in the last place above the previous unit's prefix)
                         if (z < 0) z = row_last_nonzero(p.theta, m_rs[i], m_rs[i] + kUnit * (m_cum[i + 1] - c0));
                     } else {
-                        z = tiny ? dense_search_tiny(qc, K, T - S, s_tk, s_tdc, s_tm)
-                                 : dense_bucket_search<1>(qc, K, T - S, 0, 0u, lane);
+                        z = tiny ? dense_search_tiny_blocks(ph, qb, K, p.alpha, T - S, s_tk, s_tdc, s_tm)
+                                 : dense_search_blocks(ph, qb, K, p.alpha, T - S);
                     }
                     if (z < 0) {
                         atomicOr(p.error, kErrRowRange);
@@ -926,8 +996,8 @@ __global__ void __launch_bounds__(kSampleThreads, MINB) sample_flat_kernel(const
 }
 
 size_t sample_smem_bytes(int k, int group_lanes) {
-    if (group_lanes == kFlatLanes)  // ph[pow2(K)] + qc[K] + per warp: unit prefixes and segment data
-        return ((size_t)k + (size_t)pow2_ceil(k) + (size_t)kFlatWarps * flat_unit_budget(k) +
+    if (group_lanes == kFlatLanes)  // ph[pow2(K)] + qb[K/8] + per warp: unit prefixes and segment data
+        return ((size_t)k / kDenseBlock + (size_t)pow2_ceil(k) + (size_t)kFlatWarps * flat_unit_budget(k) +
                 (size_t)kFlatWarps * kFlatMeta) *
                sizeof(float);
     // ph[pow2(K)] + inv[K] + qc[K] + the per-group running sums

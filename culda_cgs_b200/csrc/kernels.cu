@@ -11,8 +11,9 @@
 //   finalize_ll_kernel   fixed-order sum of the per-item log terms
 //   theta_rebuild_kernel block per long doc, warp per other doc (longest
 //                        first): 16-bit shared-memory histogram of the doc's
-//                        new topics, CSR compaction in ascending topic, zero
-//                        padding, n_k as a column sum.
+//                        new topics (docs of at most 32 tokens: match groups
+//                        in registers), CSR compaction in ascending topic,
+//                        zero padding, n_k as a column sum.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -123,6 +124,49 @@ __device__ __forceinline__ void theta_compact(int K, int d, int64_t len, int lan
     }
 }
 
+// One warp, a doc of at most 32 tokens: no histogram.  Each lane holds one
+// token's topic; the lanes with equal topics form a match group whose lowest
+// lane writes the entry (topic, group size) at its rank among the groups'
+// topics, so the row comes out in ascending topic order as theta_compact
+// leaves it.
+__device__ __forceinline__ void theta_short(int K, int d, int64_t b, int len, int lane,
+                                            const int32_t *__restrict__ doc_tok,
+                                            const uint16_t *__restrict__ topics, uint32_t *nk_acc, int2 *rows,
+                                            ThetaEntry *theta, int64_t &my_rows, int64_t &my_nnz,
+                                            int64_t &my_tok_nnz, int32_t *error) {
+    uint32_t z = 0xFFFFFFFFu;
+    if (lane < len) {
+        const uint32_t t = topics[doc_tok[b + lane]];
+        if (t < (uint32_t)K)
+            z = t;
+        else
+            atomicOr(error, kErrTopicRange);
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, z);
+    const bool lead = z != 0xFFFFFFFFu && __ffs(grp) - 1 == lane;
+    const int nnz = __popc(__ballot_sync(0xffffffffu, lead));
+    const uint32_t key = lead ? z : 0xFFFFFFFFu;
+    int rank = 0;
+#pragma unroll 8
+    for (int j = 0; j < 32; ++j) rank += __shfl_sync(0xffffffffu, key, j) < key;
+    const int2 row = rows[d];
+    const int start = row.x, old_end = row.y;
+    if (lead) {
+        const uint32_t c = (uint32_t)__popc(grp);
+        theta[start + rank] = theta_entry(z, c);
+        atomicAdd(&nk_acc[z], c);
+    }
+    const int new_end = start + ((nnz + 31) & ~31);
+    const int zend = max(new_end, old_end);
+    for (int j = start + nnz + lane; j < zend; j += 32) theta[j] = 0u;
+    if (lane == 0) {
+        rows[d].y = new_end;
+        my_rows += (int64_t)len * (new_end - start);
+        my_nnz += nnz;
+        my_tok_nnz += (int64_t)len * nnz;
+    }
+}
+
 }  // namespace
 
 __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
@@ -171,6 +215,11 @@ __global__ void __launch_bounds__(kThetaWarps * 32) theta_rebuild_kernel(
         const int64_t b = doc_ptr[d], e = doc_ptr[d + 1];
         if (e - b > 65535) {
             if (lane == 0) atomicOr(error, kErrLongDoc);
+            continue;
+        }
+        if (e - b <= 32) {
+            theta_short(K, d, b, (int)(e - b), lane, doc_tok, topics, nk_acc, rows, theta, my_rows, my_nnz,
+                        my_tok_nnz, error);
             continue;
         }
         theta_count(K, b, e, lane, 32, doc_tok, topics, cnt, mask, error);

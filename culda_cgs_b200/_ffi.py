@@ -127,6 +127,7 @@ SIGNATURES = {
     "culda_get_info": (C.c_int, [C.c_void_p, P(Info)]),
     "culda_last_error": (C.c_char_p, [C.c_void_p]),
     "culda_destroy": (None, [C.c_void_p]),
+    "culda_trim_memory": (C.c_int, [i32]),
     "culda_build_items": (i64, [i32, P(i64), i32, P(Item), i64, P(i32)]),
     "culda_build_segments": (i64, [i64, P(i32), P(Item), i32, i32, P(i32), i64]),
     "culda_update_phi": (C.c_int, [i32, i32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -50,6 +50,7 @@ struct culda_ctx {
     culda::DevStats *h_stats = nullptr;  // pinned (a slot of the process-wide pool)
     char *d_block = nullptr;             // every buffer above that culda_create allocates, in one allocation
     size_t block_bytes = 0;
+    bool block_pooled = false;           // d_block came from the device's block pool (freed back to it)
 
     int sample_grid = 1, theta_grid = 1;
     // theta rebuild bins: docs of at least theta_min_len tokens (the first

@@ -299,7 +299,16 @@ typedef struct culda_info {
 int culda_get_info(const culda_ctx *ctx, culda_info *info);
 
 const char *culda_last_error(const culda_ctx *ctx);
+
+/* Frees the context.  Its device block goes back to a per-device memory pool
+ * that keeps it reserved for the process, so the next culda_create on that
+ * device reuses the memory instead of mapping new pages (the reference frees
+ * each buffer with cudaFree, e.g. src_culda/model/doc_chunk.cpp:281-289). */
 void culda_destroy(culda_ctx *ctx);
+
+/* Returns the pool's unused reserve on `device` to the driver (memory that
+ * live contexts hold is untouched).  No reference counterpart. */
+int culda_trim_memory(int32_t device);
 
 /* ------------------------------------------------------------- kernel level */
 /* A sampler work item: tokens [begin, begin+count) of one word.  Words with

@@ -41,6 +41,11 @@ def test_version_and_status_strings():
     assert lib.culda_status_string(-8) == b"no CUDA device"
 
 
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the status without a device")
+def test_trim_memory_without_a_device():
+    assert cb.lib().culda_trim_memory(0) == _ffi.CULDA_ERR_NO_DEVICE
+
+
 def _params(**kw):
     d = dict(k=64, alpha=0.1, beta=0.01, seed=1, device=0, group_lanes=0, item_tokens=0, flags=0, sample_blocks=0)
     d.update(kw)

@@ -378,28 +378,43 @@ def common_config(wl, num_tokens: int, num_docs: int, num_words: int, seed: int,
 
 def measure_uneven(args, device) -> dict:
     """The batched uneven workload (118M tokens, Pareto document lengths up
-    to 50k, V = 1M) at K = 1024 with the autotuner on: the sampler variant and
-    the theta rebuild's bin threshold it chose, and the iteration times after
-    tuning (iterations 4-8, CUDA events)."""
+    to 50k, V = 1M) with the autotuner on: at K = 1024 the sampler variant and
+    the theta rebuild's bin threshold it chose and the iteration times after
+    tuning (iterations 4-8, CUDA events); then the rest of the configuration's
+    K sweep (256, 2048, 4096, alpha = 50/K) on the same corpus, iterations 4-6
+    each, as flat k<K>_* keys."""
     import culda_cgs_b200 as cb
     from culda_cgs_b200.configs import UNEVEN
 
     wl = UNEVEN.with_seed(args.seed)
     c = cb.Corpus.generate(wl.gen)
-    with cb.LDA(c, wl.k, wl.alpha, wl.beta, seed=args.seed, device=device, flags=cb.CULDA_FLAG_AUTOTUNE) as m:
-        m.iterate(3)  # the autotuner times the variants before iteration 3
-        st = m.iterate(5)
-        info = m.info()
+
+    def run(k, steps):
+        with cb.LDA(c, k, 50.0 / k, wl.beta, seed=args.seed, device=device, flags=cb.CULDA_FLAG_AUTOTUNE) as m:
+            m.iterate(3)  # the autotuner times the variants before iteration 3
+            return m.iterate(steps), m.info()
+
+    st, info = run(wl.k, 5)
     sec = [x["seconds"] for x in st]
-    return {"workload": wl.name, "num_tokens": c.num_tokens, "num_docs": c.num_docs, "k": wl.k,
-            "autotuned": bool(info["tuned"]), "group_lanes": info["group_lanes"],
-            "sample_blocks": info["sample_blocks"], "theta_min_len": info["theta_min_len"],
-            "theta_long_docs": info["theta_long_docs"], "sampler_tune_ms": round(info["tune_ms"], 4),
-            "rebuild_tune_ms": round(info["theta_tune_ms"], 4),
-            "ms_per_iteration": round(1e3 * statistics.mean(sec), 4),
-            "sample_ms": round(1e3 * statistics.mean(x["sample_seconds"] for x in st), 4),
-            "rebuild_ms": round(1e3 * statistics.mean(x["rebuild_seconds"] for x in st), 4),
-            "tokens_per_sec": round(c.num_tokens / statistics.mean(sec), 1)}
+    out = {"workload": wl.name, "num_tokens": c.num_tokens, "num_docs": c.num_docs, "k": wl.k,
+           "autotuned": bool(info["tuned"]), "group_lanes": info["group_lanes"],
+           "sample_blocks": info["sample_blocks"], "theta_min_len": info["theta_min_len"],
+           "theta_long_docs": info["theta_long_docs"], "sampler_tune_ms": round(info["tune_ms"], 4),
+           "rebuild_tune_ms": round(info["theta_tune_ms"], 4),
+           "ms_per_iteration": round(1e3 * statistics.mean(sec), 4),
+           "sample_ms": round(1e3 * statistics.mean(x["sample_seconds"] for x in st), 4),
+           "rebuild_ms": round(1e3 * statistics.mean(x["rebuild_seconds"] for x in st), 4),
+           "tokens_per_sec": round(c.num_tokens / statistics.mean(sec), 1)}
+    for k in args.uneven_ks:
+        st, info = run(k, 3)
+        ms = 1e3 * statistics.mean(x["seconds"] for x in st)
+        out[f"k{k}_ms_per_iteration"] = round(ms, 4)
+        out[f"k{k}_sample_ms"] = round(1e3 * statistics.mean(x["sample_seconds"] for x in st), 4)
+        out[f"k{k}_rebuild_ms"] = round(1e3 * statistics.mean(x["rebuild_seconds"] for x in st), 4)
+        out[f"k{k}_tokens_per_sec"] = round(c.num_tokens / (ms / 1e3), 1)
+        out[f"k{k}_variant"] = f"G={info['group_lanes']} blocks={info['sample_blocks']} " \
+                               f"theta_min_len={info['theta_min_len']}"
+    return out
 
 
 # ------------------------------------------------------------------- ours
@@ -756,6 +771,8 @@ def main():
     ap.add_argument("--ref-timeout", type=float, default=1200.0)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-form and fold-in measurements")
     ap.add_argument("--no-uneven", action="store_true", help="skip the autotuned uneven-workload measurement")
+    ap.add_argument("--uneven-ks", type=lambda v: [int(x) for x in v.split(",") if x], default=[256, 2048, 4096],
+                    help="the rest of the uneven workload's K sweep, measured after K = 1024 (empty: none)")
     ap.add_argument("--learned-epochs", type=int, default=8)
     ap.add_argument("--learned-batch", type=int, default=1024)
     args = ap.parse_args()

@@ -918,7 +918,7 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
                         need_seg <= size - o_after_seg;
     if (!borrow) {
         arena.size = std::max(std::max(need_check, need_order), std::max(need_rev, need_seg));
-        CKB(cudaMalloc((void **)&arena.base, arena.size));
+        CKB((cudaError_t)device_malloc((void **)&arena.base, arena.size));
         arena.owned = true;
     }
     // the arena for a phase that may use the block from offset `from` on
@@ -1357,6 +1357,23 @@ extern "C" const char *culda_status_string(int status) {
         default: return "unknown status";
     }
 }
+
+namespace culda {
+int device_malloc(void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaErrorMemoryAllocation) return (int)e;
+    cudaGetLastError();
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kPoolDevices) return (int)e;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        pool = g_pools[dev];
+    }
+    if (!pool || cudaMemPoolTrimTo(pool, 0) != cudaSuccess) return (int)e;
+    return (int)cudaMalloc(p, bytes);
+}
+}  // namespace culda
 
 extern "C" int culda_trim_memory(int32_t device) {
     int ndev = 0;

@@ -364,7 +364,8 @@ namespace {
 
 template <class T>
 cudaError_t ealloc(culda_encoder *e, T **p, size_t n) {
-    cudaError_t r = cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(n, 1) * sizeof(T));
+    const cudaError_t r =
+        (cudaError_t)device_malloc(reinterpret_cast<void **>(p), std::max<size_t>(n, 1) * sizeof(T));
     if (r == cudaSuccess) e->allocs.push_back(*p);
     return r;
 }

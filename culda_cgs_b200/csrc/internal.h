@@ -20,6 +20,11 @@ bool read_file_bytes(const std::string &path, std::vector<char> &buf);
 // Host checks of a corpus descriptor (prefix arrays, doc ids, doc lengths).
 int validate_corpus(const culda_corpus *c);
 
+// cudaMalloc on the current device; when it runs out of memory, the
+// context-block pool's unused reserve on that device is handed back and the
+// allocation is tried once more (returns the CUDA status).
+int device_malloc(void **p, size_t bytes);
+
 // Device error word bits.
 enum : int32_t {
     kErrTopicRange = 1,   // a topic >= K was found in the topic array

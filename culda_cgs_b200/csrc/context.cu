@@ -831,11 +831,18 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     // region holds their temporaries instead of an allocation of its own.
     auto rnd = [](size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255; };
     size_t t_order = 0, t_doc = 0, t_scan = 0, t_sum = 0;
-    int order_bits = 17, doc_bits = 1;
-    while ((1ll << (order_bits - 16)) < (int64_t)V) ++order_bits;
+    // token-order keys: 32-bit (word, 8-bit length class) up to 2^24 words, else
+    // 64-bit (word, exact length); the 32-bit sort moves a third of the bytes
+    const bool key32 = V <= (1 << 24);
+    int order_bits = key32 ? 9 : 17, doc_bits = 1;
+    while ((1ll << (order_bits - (key32 ? 8 : 16))) < (int64_t)V) ++order_bits;
     while ((1ll << doc_bits) < (int64_t)D) ++doc_bits;
-    CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_order, (const uint64_t *)nullptr, (uint64_t *)nullptr,
-                                        (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, order_bits, s));
+    if (key32)
+        CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_order, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, order_bits, s));
+    else
+        CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_order, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, order_bits, s));
     CKB(cub::DeviceRadixSort::SortPairs(nullptr, t_doc, (const int32_t *)nullptr, (int32_t *)nullptr,
                                         (const int32_t *)nullptr, (int32_t *)nullptr, (int)N, 0, doc_bits, s));
     CKB(cub::DeviceScan::InclusiveScan(nullptr, t_scan, (const int32_t *)nullptr, (int32_t *)nullptr, MaxOp(), (int)N,
@@ -843,7 +850,8 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     CKB(cub::DeviceScan::ExclusiveSum(nullptr, t_sum, (const int32_t *)nullptr, (int32_t *)nullptr, (int)N + 1, s));
     // what each set-up phase takes from the arena (SetupArena rounds like rnd)
     const size_t need_check = rnd(sizeof(int32_t) * (size_t)D);
-    const size_t need_order = reorder ? 2 * rnd(sizeof(uint64_t) * (size_t)N) + rnd(sizeof(int32_t) * (size_t)N) +
+    const size_t key_bytes = key32 ? sizeof(uint32_t) : sizeof(uint64_t);
+    const size_t need_order = reorder ? 2 * rnd(key_bytes * (size_t)N) + rnd(sizeof(int32_t) * (size_t)N) +
                                             rnd(t_order)
                                       : 0;
     const size_t need_rev = 2 * rnd(sizeof(int32_t) * (size_t)N) + rnd(t_doc);
@@ -998,24 +1006,36 @@ extern "C" int culda_create(const culda_corpus *c, const culda_params *p, culda_
     mark("upload, doc check");
 
     // Stored token order: inside each word, tokens sorted by their doc's
-    // length, longest first (a stable sort on (word, 65535 - L_d) keeps doc
-    // order among equal lengths).  Neighbouring segments then walk theta rows
+    // length, longest first (a stable sort on (word, length class of L_d), or
+    // on (word, 65535 - L_d) past 2^24 words, keeps doc order among equal
+    // keys).  Neighbouring segments then walk theta rows
     // of similar length.  Sampling results do not depend on this order:
     // each token's Philox stream is keyed on its input index.
     if (reorder) {
         arena_at(o_late);
-        uint64_t *keys = arena.take<uint64_t>((size_t)N), *keys_out = arena.take<uint64_t>((size_t)N);
+        char *keys = arena.take<char>(key_bytes * (size_t)N), *keys_out = arena.take<char>(key_bytes * (size_t)N);
         int32_t *vals = arena.take<int32_t>((size_t)N);
         const int end_bit = order_bits;
         size_t tmp_bytes = 0;
-        CKA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
-                                            end_bit, s));
+        if (key32)
+            CKA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint32_t *)keys, (uint32_t *)keys_out, vals,
+                                                ctx->d_tok_index, (int)N, 0, end_bit, s));
+        else
+            CKA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint64_t *)keys, (uint64_t *)keys_out, vals,
+                                                ctx->d_tok_index, (int)N, 0, end_bit, s));
         void *tmp = arena.take<char>(tmp_bytes);
         if (!keys || !keys_out || !vals || !tmp) CKA(cudaErrorMemoryAllocation);
-        CKA(launch_order_keys(V, N, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, keys, s));
+        if (key32)
+            CKA(launch_order_keys32(V, N, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, (uint32_t *)keys, s));
+        else
+            CKA(launch_order_keys(V, N, ctx->d_word_ptr, ctx->d_doc_ids, ctx->d_doc_ptr, (uint64_t *)keys, s));
         CKA(launch_iota(N, vals, s));
-        CKA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_out, vals, ctx->d_tok_index, (int)N, 0,
-                                            end_bit, s));
+        if (key32)
+            CKA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, (uint32_t *)keys, (uint32_t *)keys_out, vals,
+                                                ctx->d_tok_index, (int)N, 0, end_bit, s));
+        else
+            CKA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, (uint64_t *)keys, (uint64_t *)keys_out, vals,
+                                                ctx->d_tok_index, (int)N, 0, end_bit, s));
         // the doc ids in the stored order, through the (now free) key buffer
         int32_t *ids2 = reinterpret_cast<int32_t *>(keys);
         CKA(launch_gather<int32_t>(N, ctx->d_tok_index, ctx->d_doc_ids, ids2, s));

@@ -361,6 +361,42 @@ cudaError_t launch_order_keys(int num_words, int64_t num_tokens, const int64_t *
     return cudaGetLastError();
 }
 
+// 32-bit keys for vocabularies of at most 2^24 words: the word above an 8-bit
+// log-linear length class, 16 classes per doubling (the position of the
+// length's leading one and the 4 bits after it), longest first.  Docs in one
+// class keep their input order (the sort is stable), so a doc's tokens inside
+// a word stay contiguous.
+__global__ void order_keys32_kernel(int num_words, int64_t num_tokens, const int64_t *__restrict__ word_ptr,
+                                    const int32_t *__restrict__ doc_ids, const int64_t *__restrict__ doc_ptr,
+                                    uint32_t *keys) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < num_tokens;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = num_words - 1;  // the last word w with word_ptr[w] <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(word_ptr + mid) <= t)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const int d = doc_ids[t];
+        const int64_t l64 = doc_ptr[d + 1] - doc_ptr[d];
+        const uint32_t len = l64 < 1 ? 1u : l64 > 65535 ? 65535u : (uint32_t)l64;
+        const uint32_t msb = 31u - __clz(len);                         // 0 .. 15
+        const uint32_t frac = ((len << (31u - msb)) >> 27) & 15u;      // the 4 bits after the leading one
+        keys[t] = ((uint32_t)lo << 8) | (255u - (msb * 16u + frac));
+    }
+}
+
+cudaError_t launch_order_keys32(int num_words, int64_t num_tokens, const int64_t *word_ptr, const int32_t *doc_ids,
+                                const int64_t *doc_ptr, uint32_t *keys, cudaStream_t s) {
+    if (num_tokens <= 0) return cudaSuccess;
+    if (num_words > (1 << 24)) return cudaErrorInvalidValue;
+    order_keys32_kernel<<<grid_for(num_tokens), 256, 0, s>>>(num_words, num_tokens, word_ptr, doc_ids, doc_ptr,
+                                                             keys);
+    return cudaGetLastError();
+}
+
 template <class T>
 __global__ void gather_kernel(int64_t n, const int32_t *__restrict__ index, const T *__restrict__ src, T *dst) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

@@ -125,6 +125,10 @@ cudaError_t launch_loglik_joint(int k, int num_words, int num_docs, float alpha,
 // (longest first, doc id breaking ties).  keys[t] = (word << 16) | (65535 - L).
 cudaError_t launch_order_keys(int num_words, int64_t num_tokens, const int64_t *word_ptr, const int32_t *doc_ids,
                               const int64_t *doc_ptr, uint64_t *keys, cudaStream_t s);
+// The same order with 32-bit keys (num_words <= 2^24): keys[t] = (word << 8) |
+// (255 - length class), 16 classes per doubling of L.
+cudaError_t launch_order_keys32(int num_words, int64_t num_tokens, const int64_t *word_ptr, const int32_t *doc_ids,
+                                const int64_t *doc_ptr, uint32_t *keys, cudaStream_t s);
 template <class T>
 cudaError_t launch_gather(int64_t n, const int32_t *index, const T *src, T *dst, cudaStream_t s);
 template <class T>

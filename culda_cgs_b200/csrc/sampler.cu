@@ -5,12 +5,14 @@
 // item the word's phi row is built as a shared-memory histogram of the
 // snapshot topics (no dense V x K phi in HBM), phihat = (n_wk + beta) /
 // (n_k + V beta) is formed in FP32 at shared-memory offset 0, and the
-// alpha*phihat prefix of the dense bucket is scanned.  The item's tokens come
+// alpha*phihat prefix of the dense bucket is scanned (by the flat sampler
+// once per block of 8 topics).  The item's tokens come
 // in segments (runs of one doc, at most 32 tokens) that share one walk of the
 // doc's theta row and differ only in their Philox uniforms.  Two samplers do
 // the walks and draws:
 //   sample_flat_kernel (the default): a warp splits the rows of a batch of
-//     segments evenly over 8 groups of 4 lanes, builds every row's prefix
+//     segments evenly over 8 groups of 4 lanes (one 256-bit load per lane
+//     per step, two alternating prefetch buffers), builds every row's prefix
 //     sums in shared memory, and each lane then draws its own tokens;
 //   sample_kernel<G>: a group of G lanes walks one row with 32-byte loads
 //     (8 entries per lane per step), keeps the running sum after every step

@@ -118,6 +118,37 @@ def test_build_items_splits_hot_words_and_covers_every_token():
     assert sum(it[4] for it in items) == int((lens > 0).sum())  # one first item per non-empty word
 
 
+def _items_reference(lens, item_tokens):
+    """Words in order, words longer than item_tokens cut into ns slices of
+    ceil(len / ns) tokens (the last shorter), then a stable sort by size,
+    largest first."""
+    out, hot, off = [], 0, 0
+    for w, n in enumerate(lens):
+        if n > item_tokens:
+            ns = -(-n // item_tokens)
+            sz = -(-n // ns)
+            for i in range(ns):
+                b, e = off + i * sz, min(off + (i + 1) * sz, off + n)
+                if e > b:
+                    out.append((b, e - b, w, hot, 1 if i == 0 else 0))
+            hot += 1
+        elif n > 0:
+            out.append((off, n, w, -1, 1))
+        off += n
+    return sorted(out, key=lambda x: -x[1]), hot
+
+
+@pytest.mark.parametrize("item_tokens", [7, 300, 4096])
+def test_build_items_matches_a_stable_sort_of_the_slices(item_tokens):
+    rng = np.random.default_rng(item_tokens)
+    lens = rng.zipf(1.3, size=3000).clip(0, 20000) * rng.integers(0, 2, size=3000)
+    wp = np.concatenate([[0], np.cumsum(lens)])
+    items, nhot = build_items(wp, item_tokens)
+    ref, ref_hot = _items_reference([int(x) for x in lens], item_tokens)
+    assert nhot == ref_hot
+    assert items == ref
+
+
 def test_build_segments_runs_of_one_doc_inside_items():
     lens = np.array([70, 5, 1, 40])
     wp = np.concatenate([[0], np.cumsum(lens)])
